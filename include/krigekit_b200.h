@@ -1,0 +1,120 @@
+/*
+ * krigekit_b200.h -- C-ABI of libkrigecuda.so, the B200 kriging solve path.
+ *
+ * The krige_* entry points keep the names, argument order, array layouts
+ * (Fortran column-major, 1-based variable indices) and error convention of
+ * the reference engine's ISO_C_BINDING layer (ougx/krigekit
+ * src/libkriging/kriging_capi.F90, kriging_capi_common.F90): every function
+ * returns 0 on success and 1 on error, with the message available through
+ * krige_get_last_error().  A caller that binds the reference library with
+ * ctypes (src/krigekit/kriging.py:142-286) can bind this library instead.
+ * Inputs are copied at each set_* call; outputs go to caller buffers.
+ * Device memory is allocated by the library (cudaMalloc, or the allocator
+ * registered with krige_set_allocator).
+ */
+#ifndef KRIGEKIT_B200_H
+#define KRIGEKIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* kriging_capi.F90:43-57 krige_create: new handle (1-based registry slot). */
+int krige_create(int64_t *handle);
+/* kriging_capi_common.F90 krige_destroy (release_obj_base): frees device and host state. */
+int krige_destroy(int64_t *handle);
+
+/* kriging_capi.F90:143-192 krige_initialize -> initialize_base (kriging_base.F90:467-553).
+ * nsim > 0, use_old_weight, store_weight, weight_correction and varying_vgm are
+ * outside the GPU kriging path and return an error. */
+int krige_initialize(int64_t handle, int ndim, int nvar, int ndrift, int unbias, int nsim,
+                     int anisotropic_search, int weight_correction, int use_old_weight,
+                     int store_weight, int cross_validation, int write_mat, int neglect_error,
+                     int varying_vgm, int std_ck, int verbose, int pf_cache,
+                     const char *weight_file, const double *bounds /* [2] */, int seed);
+
+/* kriging_capi.F90:197-224 krige_set_obs: coord(ndim_c, nobs), value(nobs), variance(nobs). */
+int krige_set_obs(int64_t handle, int ivar, int nobs, int ndim_c, const double *coord,
+                  const double *value, const double *variance, int nmax, double maxdist,
+                  double sk_mean);
+/* kriging_capi.F90 krige_update_obs_value -> update_obs_value_base (kriging_base.F90:649-680). */
+int krige_update_obs_value(int64_t handle, int ivar, int nobs, const double *value);
+/* kriging_capi.F90 krige_set_obs_drift: drift(ndrift_c, nobs). */
+int krige_set_obs_drift(int64_t handle, int ivar, int ndrift_c, int nobs, const double *drift);
+
+/* kriging_capi.F90:230-243 krige_reset_vgm. */
+int krige_reset_vgm(int64_t handle, int ivar, int jvar);
+/* kriging_capi.F90:245-268 krige_set_vgm -> set_vgm (kriging.F90:211-276); jvar >= ivar. */
+int krige_set_vgm(int64_t handle, int ivar, int jvar, const char *vtype, double nugget,
+                  double sill, double a_major, double a_minor1, double a_minor2,
+                  double azimuth, double dip, double plunge, int is_product);
+
+/* kriging_capi.F90:310-331 krige_set_grid: coord(ndim_c, ngrid), rangescale/localnugget(ngrid). */
+int krige_set_grid(int64_t handle, int ngrid, int ndim_c, const double *coord,
+                   const double *rangescale, const double *localnugget);
+/* kriging_capi.F90:334-378 krige_set_grid_block: block_type -4 (Gauss quadrature,
+ * coord = centres, blocksize(ndim_c, nblock)) or > 0 (coord = nodes, nblockpnt, pointweight). */
+int krige_set_grid_block(int64_t handle, int block_type, int ngrid, int ndim_c,
+                         const double *coord, int nblock, const int *nblockpnt,
+                         const double *pointweight, const double *blocksize,
+                         const double *rangescale, const double *localnugget);
+/* kriging_capi.F90 krige_set_grid_cv -> set_grid_cv_base (kriging_base.F90:1120-1135). */
+int krige_set_grid_cv(int64_t handle);
+/* kriging_capi.F90:380-397 krige_set_grid_drift: drift(ndrift_c, nblocks); ivar < 0 = all. */
+int krige_set_grid_drift(int64_t handle, int ivar, int ndrift_c, int nblocks, const double *drift);
+
+/* kriging_capi.F90:448-467 krige_set_search -> set_search (kriging.F90:318-387). */
+int krige_set_search(int64_t handle, int ivar, double anis1, double anis2, double azimuth,
+                     double dip, double plunge, int sector_search);
+
+/* kriging_capi_common.F90:229-239 krige_solve -> solve_base (kriging_base.F90:2064-2194).
+ * nthread and ncache (CPU threads, factor-cache slots) are accepted and ignored. */
+int krige_solve(int64_t handle, int nthread, int ncache);
+/* kriging_capi_common.F90:113-128 krige_solver_stats: out[5] = fail, chol_fact,
+ * chol_reuse, ssytrf_fact, ssytrf_reuse (the GPU solves every target: no reuse). */
+void krige_solver_stats(int64_t handle, int *out);
+/* kriging_capi_common.F90:90-96 krige_get_last_error. */
+int krige_get_last_error(char *buffer, int nbuf);
+
+/* kriging_capi_common.F90 krige_get_nblocks / krige_get_nsim. */
+int krige_get_nblocks(int64_t handle, int *nblocks);
+int krige_get_nsim(int64_t handle, int *nsim);
+/* kriging_capi_common.F90:277-288 krige_get_block_coord: out(ndim_c, nblocks). */
+int krige_get_block_coord(int64_t handle, int ndim_c, int nblocks, double *out);
+/* kriging_capi_common.F90:290-306 krige_get_estimate: out(nblocks, nsim_c), variable 1. */
+int krige_get_estimate(int64_t handle, int nsim_c, int nblocks, double *out);
+/* kriging_capi_common.F90:323-344 krige_get_estimate_all: out(nblocks, nvar_c, nsim_c). */
+int krige_get_estimate_all(int64_t handle, int nblocks, int nvar_c, int nsim_c, double *out);
+/* kriging_capi_common.F90:352-369 krige_get_variance: out(nblocks), variable 1. */
+int krige_get_variance(int64_t handle, int nblocks, double *out);
+/* kriging_capi_common.F90:372-392 krige_get_variance_all: out(nblocks, nvar_c, nvar_c). */
+int krige_get_variance_all(int64_t handle, int nblocks, int nvar_c, double *out);
+
+/* ---- extensions of the GPU library (no counterpart in the reference) ---- */
+/* 0 = FP64 throughout, 1 = FP32 factorisation with FP64 iterative refinement (default). */
+int krige_set_precision(int64_t handle, int mode);
+/* Targets with fewer than nmin neighbours return NaN (0 = reference behaviour). */
+int krige_set_nmin(int64_t handle, int nmin);
+/* CUDA device ordinal and cudaStream_t used by this handle. */
+int krige_set_device(int64_t handle, int device, void *stream);
+/* Route device allocations through caller callbacks (e.g. a framework allocator). */
+void krige_set_allocator(void *(*alloc)(size_t bytes, void *ctx), void (*release)(void *ptr, void *ctx),
+                         void *ctx);
+/* Neighbour sets of the last solve: nnear(nblocks), inear(mmax, nblocks), 1-based ascending. */
+int krige_get_neighbours(int64_t handle, int ivar, int nblocks, int mmax, int *nnear, int *inear);
+/* Leading dimension of the neighbour list of variable ivar. */
+int krige_get_mmax(int64_t handle, int ivar, int *mmax);
+/* Per-target status bits of the last solve (tie/overflow search fallback, FP64
+ * re-solve, LDL^T path, failure, no neighbours). */
+int krige_get_status(int64_t handle, int nblocks, int *status);
+/* Counters of the last solve: out8 = fail, cholesky, 0, ldlt, 0, search fallbacks,
+ * FP64 re-solves, refinement iterations; solve_ms = wall time of krige_solve. */
+int krige_gpu_stats(int64_t handle, int *out8, double *solve_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

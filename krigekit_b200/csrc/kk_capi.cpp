@@ -1,0 +1,609 @@
+// kk_capi.cpp -- the krige_* C-ABI of libkrigecuda.so.
+//
+// Entry points keep the names, argument order, array layouts (Fortran
+// column-major) and error convention (int32 ierr, 0 = ok; message through
+// krige_get_last_error) of the reference's ISO_C_BINDING layer
+// (src/libkriging/kriging_capi.F90, kriging_capi_common.F90,
+// kriging_st_capi.f90), so the reference's ctypes wrapper can bind this
+// library unchanged for the kriging path.  Each function cites the
+// reference routine it replaces; declarations live in include/krigekit_b200.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kk_host.h"
+
+namespace kk {
+
+static std::string g_err;
+static std::mutex g_err_mu;
+
+void set_error(const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  if (g_err.empty()) g_err = msg;
+}
+void clear_error() {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_err.clear();
+}
+bool failed() {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return !g_err.empty();
+}
+
+static std::vector<std::unique_ptr<Engine>> g_reg;
+static std::mutex g_reg_mu;
+
+static Engine* get(int64_t h) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  if (h < 1 || h > (int64_t)g_reg.size() || !g_reg[h - 1]) {
+    set_error("invalid kriging handle");
+    return nullptr;
+  }
+  return g_reg[h - 1].get();
+}
+
+static int ierr() { return failed() ? 1 : 0; }
+
+static int vtype_id(const char* s) {
+  // vtype_from_str, vgmfunc.f90:83-99 (case-insensitive 3-character prefix)
+  static const char* names[] = {"nug", "sph", "exp", "gau", "hol", "pow", "bsq", "cir", "lin", "cyc", "dco"};
+  char b[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 3 && s && s[i]; ++i) b[i] = (char)std::tolower((unsigned char)s[i]);
+  for (int k = 0; k < 11; ++k)
+    if (std::strncmp(b, names[k], 3) == 0) return k;
+  return -1;
+}
+
+}  // namespace kk
+
+using namespace kk;
+
+#define KK_GUARD_BEGIN \
+  clear_error();       \
+  try {
+#define KK_GUARD_END                           \
+  }                                            \
+  catch (const std::string& m) { set_error(m); } \
+  catch (const std::exception& x) { set_error(x.what()); } \
+  return ierr();
+
+extern "C" {
+
+// krige_create, kriging_capi.F90:43-57
+int krige_create(int64_t* handle) {
+  KK_GUARD_BEGIN
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  g_reg.emplace_back(new Engine());
+  *handle = (int64_t)g_reg.size();
+  KK_GUARD_END
+}
+
+// krige_destroy, kriging_capi_common.F90 (release_obj_base)
+int krige_destroy(int64_t* handle) {
+  KK_GUARD_BEGIN
+  Engine* e = get(*handle);
+  if (e) {
+    engine_release(*e);
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_reg[*handle - 1].reset();
+  }
+  *handle = 0;
+  KK_GUARD_END
+}
+
+// krige_initialize, kriging_capi.F90:143-192 -> initialize_base (kriging_base.F90:467-553)
+int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int nsim, int anisotropic_search,
+                     int weight_correction, int use_old_weight, int store_weight, int cross_validation,
+                     int write_mat, int neglect_error, int varying_vgm, int std_ck, int verbose, int pf_cache,
+                     const char* weight_file, const double* bounds, int seed) {
+  (void)pf_cache; (void)weight_file; (void)seed; (void)write_mat;
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (nsim > 0) throw std::string("sequential simulation (nsim > 0) is not part of the GPU kriging path");
+  if (use_old_weight || store_weight) throw std::string("weight-file reuse is not part of the GPU kriging path");
+  if (weight_correction) throw std::string("weight_correction is not part of the GPU kriging path");
+  if (varying_vgm) throw std::string("varying_vgm is not part of the GPU kriging path");
+  if (ndim < 1 || ndim > 3) throw std::string("ndim must be 1, 2 or 3");
+  if (nvar < 1 || nvar > KK_MAXVAR) throw std::string("nvar must be 1..4");
+  engine_release(*e);
+  for (int a = 0; a < KK_MAXVAR; ++a)
+    for (int b = 0; b < KK_MAXVAR; ++b) {
+      e->vgm[a][b].clear();
+      e->vgm_t[a][b].clear();
+      e->joint[a][b].clear();
+      }
+  for (int v = 0; v < KK_MAXVAR; ++v) {
+    e->vd[v].grid_ready = false;
+    e->vd[v].tree_ready = false;
+  }
+  e->st = 0;
+  e->nblock = 0;
+  e->bcoord.clear(); e->nblockpnt.clear(); e->gcoord.clear(); e->gweight.clear();
+  e->rangescale.clear(); e->localnugget.clear(); e->bdrift.clear();
+  e->grid_dirty = true;
+  e->solved = false;
+  e->ndim = ndim;
+  e->nlag = ndim;
+  e->nvar = nvar;
+  e->ndrift = ndrift;
+  e->unbias = unbias;
+  e->nsim = nsim;
+  e->anisotropic_search = anisotropic_search;
+  e->cross_validation = cross_validation;
+  e->neglect_error = neglect_error;
+  e->std_ck = std_ck;
+  e->verbose = verbose;
+  e->bounds[0] = bounds ? bounds[0] : -DBL_MAX;
+  e->bounds[1] = bounds ? bounds[1] : DBL_MAX;
+  e->obs.assign(nvar, ObsVar());
+  KK_GUARD_END
+}
+
+// krige_set_obs, kriging_capi.F90:197-224 -> set_obs_base (kriging_base.F90:560-639)
+int krige_set_obs(int64_t h, int ivar, int nobs, int ndim_c, const double* coord, const double* value,
+                  const double* variance, int nmax, double maxdist, double sk_mean) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  if (ndim_c != e->nlag) throw std::string("nlag /= size(coord, 1) for obs");
+  ObsVar& o = e->obs[ivar - 1];
+  o = ObsVar();
+  o.n = nobs;
+  o.coord.assign(coord, coord + (size_t)ndim_c * nobs);
+  o.value.assign(value, value + nobs);
+  if (variance) o.variance.assign(variance, variance + nobs);
+  else o.variance.assign(nobs, 0.0);
+  // duplicate coordinate check (check_duplicate_coordinates_base, utils.F90:43-133)
+  {
+    std::vector<int> idx(nobs);
+    for (int i = 0; i < nobs; ++i) idx[i] = i;
+    const double* c = o.coord.data();
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) {
+      for (int k = 0; k < ndim_c; ++k) {
+        double x = c[(size_t)a * ndim_c + k], y = c[(size_t)b * ndim_c + k];
+        if (x != y) return x < y;
+      }
+      return a < b;
+    });
+    for (int i = 1; i < nobs; ++i) {
+      bool same = true;
+      for (int k = 0; k < ndim_c; ++k)
+        if (c[(size_t)idx[i] * ndim_c + k] != c[(size_t)idx[i - 1] * ndim_c + k]) { same = false; break; }
+      if (same) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "Duplicate observation coordinates at points %d and %d", idx[i - 1] + 1, idx[i] + 1);
+        o = ObsVar();
+        throw std::string(msg);
+      }
+    }
+  }
+  o.nmax = nmax;
+  o.maxdist = maxdist;
+  o.sk_mean = sk_mean;
+  o.dirty = true;
+  KK_GUARD_END
+}
+
+// krige_update_obs_value (kriging_base.F90:649-680): new values, same locations
+int krige_update_obs_value(int64_t h, int ivar, int nobs, const double* value) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  ObsVar& o = e->obs[ivar - 1];
+  if (nobs != o.n) throw std::string("size(value) /= obs%n");
+  o.value.assign(value, value + nobs);
+  bool keep_search = o.search_set;
+  o.dirty = true;
+  o.search_set = keep_search;
+  KK_GUARD_END
+}
+
+// krige_set_obs_drift, kriging_capi.F90 -> set_obs_drift_base (kriging_base.F90:718-752)
+int krige_set_obs_drift(int64_t h, int ivar, int ndrift_c, int nobs, const double* drift) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  ObsVar& o = e->obs[ivar - 1];
+  if (o.n == 0) throw std::string("Observation needs to be set before adding drift.");
+  if (e->ndrift == 0) throw std::string("Observation drift is specified but ndrift==0");
+  if (ndrift_c != e->ndrift) throw std::string("size(drift, 1) /= ndrift");
+  if (nobs != o.n) throw std::string("size(drift, 2) /= nobs");
+  o.drift.assign(drift, drift + (size_t)ndrift_c * nobs);
+  o.dirty = true;
+  KK_GUARD_END
+}
+
+// krige_reset_vgm, kriging_capi.F90:230-243
+int krige_reset_vgm(int64_t h, int ivar, int jvar) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  int a = std::min(ivar, jvar) - 1, b = std::max(ivar, jvar) - 1;
+  if (a < 0 || b >= e->nvar) throw std::string("ivar/jvar out of range");
+  e->vgm[a][b].clear();
+  KK_GUARD_END
+}
+
+// krige_set_vgm, kriging_capi.F90:245-268 -> set_vgm (kriging.F90:211-276)
+int krige_set_vgm(int64_t h, int ivar, int jvar, const char* vtype, double nugget, double sill, double a_major,
+                  double a_minor1, double a_minor2, double azimuth, double dip, double plunge, int is_product) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || jvar < 1 || ivar > e->nvar || jvar > e->nvar) throw std::string("ivar/jvar out of range");
+  if (jvar < ivar) throw std::string("jvar must be >= ivar to set the upper triangle of the variogram matrix");
+  int id = vtype_id(vtype);
+  if (id < 0) throw std::string("Unknown variogram type: ") + (vtype ? vtype : "");
+  std::vector<StructSpec>& v = e->vgm[ivar - 1][jvar - 1];
+  if (is_product && v.empty())
+    throw std::string("first structure cannot be a product member (product=.true. requires a preceding structure)");
+  if ((int)v.size() >= KK_MAXSTRUCT) throw std::string("exceeded the maximum number of nested structures");
+  StructSpec s;
+  s.vtype = id;
+  s.nugget = nugget;
+  s.sill = sill;
+  s.a_major = a_major;
+  s.a_minor1 = a_minor1;
+  s.a_minor2 = a_minor2;
+  s.az = azimuth;
+  s.dip = dip;
+  s.plunge = plunge;
+  s.is_product = is_product ? 1 : 0;
+  v.push_back(s);
+  KK_GUARD_END
+}
+
+static void grid_common(Engine* e, int nblock, const double* rangescale, const double* localnugget) {
+  e->nblock = nblock;
+  e->rangescale.clear();
+  e->localnugget.clear();
+  bool rs1 = true, ln0 = true;
+  for (int i = 0; rangescale && i < nblock; ++i) rs1 = rs1 && rangescale[i] == 1.0;
+  for (int i = 0; localnugget && i < nblock; ++i) ln0 = ln0 && localnugget[i] == 0.0;
+  if (rangescale && !rs1) e->rangescale.assign(rangescale, rangescale + nblock);
+  if (localnugget && !ln0) e->localnugget.assign(localnugget, localnugget + nblock);
+  e->bdrift.clear();
+  if (e->ndrift > 0) e->bdrift.assign((size_t)e->ndrift * e->nvar * nblock, 0.0);
+  e->grid_dirty = true;
+  e->solved = false;
+}
+
+// krige_set_grid, kriging_capi.F90:310-331 -> set_grid_point_base (kriging_base.F90:981-1004)
+int krige_set_grid(int64_t h, int ngrid, int ndim_c, const double* coord, const double* rangescale,
+                   const double* localnugget) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
+  if (ndim_c != e->nlag) throw std::string("nlag /= size(coord, 1) for self%grid");
+  e->bcoord.assign(coord, coord + (size_t)ndim_c * ngrid);
+  e->nblockpnt.clear();
+  e->gcoord.clear();
+  e->gweight.clear();
+  grid_common(e, ngrid, rangescale, localnugget);
+  KK_GUARD_END
+}
+
+// krige_set_grid_block, kriging_capi.F90:334-378: GQ blocks (set_grid_gq_base,
+// kriging_base.F90:1010-1068) or user blocks (set_grid_user_block_base)
+int krige_set_grid_block(int64_t h, int block_type, int ngrid, int ndim_c, const double* coord, int nblock,
+                         const int* nblockpnt, const double* pointweight, const double* blocksize,
+                         const double* rangescale, const double* localnugget) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
+  if (ndim_c != e->nlag) throw std::string("nlag /= size(coord, 1) for self%grid");
+  const int D = ndim_c;
+  if (block_type == -4) {
+    // Gauss-Legendre 4-point rule per axis (gaussian_quadrature.f90:1-41)
+    const double frac[4] = {0.4305681558, 0.1699905218, -0.1699905218, -0.4305681558};
+    const double wgq4[4] = {0.1739274226, 0.3260725774, 0.3260725774, 0.1739274226};
+    const int nb = ngrid;
+    int ngq = 1;
+    for (int k = 0; k < D; ++k) ngq *= 4;
+    e->bcoord.assign(coord, coord + (size_t)D * nb);
+    e->nblockpnt.assign(nb, ngq);
+    e->gcoord.assign((size_t)D * nb * ngq, 0.0);
+    e->gweight.assign((size_t)nb * ngq, 0.0);
+    for (int ib = 0; ib < nb; ++ib)
+      for (int g = 0; g < ngq; ++g) {
+        int ii[3] = {g % 4, (g / 4) % 4, g / 16};
+        double w = 1.0;
+        for (int k = 0; k < D; ++k) {
+          e->gcoord[((size_t)ib * ngq + g) * D + k] = coord[(size_t)ib * D + k] + frac[ii[k]] * blocksize[(size_t)ib * D + k];
+          w = w * wgq4[ii[k]];
+        }
+        e->gweight[(size_t)ib * ngq + g] = w;
+      }
+    grid_common(e, nb, rangescale, localnugget);
+  } else {
+    if (block_type <= 0) throw std::string("block_type must be >0 for user block grids.");
+    long long tot = 0;
+    for (int i = 0; i < nblock; ++i) {
+      if (nblockpnt[i] <= 0) throw std::string("nblockpnt entries must be positive");
+      tot += nblockpnt[i];
+    }
+    if (tot != ngrid) throw std::string("gridcoord columns != sum(nblockpnt)");
+    e->nblockpnt.assign(nblockpnt, nblockpnt + nblock);
+    e->gcoord.assign(coord, coord + (size_t)D * ngrid);
+    if (pointweight) e->gweight.assign(pointweight, pointweight + ngrid);
+    else {
+      e->gweight.resize(ngrid);
+      size_t g = 0;
+      for (int i = 0; i < nblock; ++i)
+        for (int k = 0; k < nblockpnt[i]; ++k) e->gweight[g++] = 1.0 / nblockpnt[i];
+    }
+    // weighted centroid (set_grid_centroid_common, kriging_base.F90:1546-1560)
+    e->bcoord.assign((size_t)D * nblock, 0.0);
+    size_t g0 = 0;
+    for (int ib = 0; ib < nblock; ++ib) {
+      const int nn = nblockpnt[ib];
+      double denom = 0.0;
+      for (int k = 0; k < nn; ++k) denom = denom + e->gweight[g0 + k];
+      if (denom <= 0.0) throw std::string("sum(pointweight) must be positive for every block");
+      for (int d = 0; d < D; ++d) {
+        double s = 0.0;
+        for (int k = 0; k < nn; ++k) s = s + e->gcoord[(g0 + k) * D + d] * e->gweight[g0 + k];
+        e->bcoord[(size_t)ib * D + d] = s / denom;
+      }
+      g0 += nn;
+    }
+    grid_common(e, nblock, rangescale, localnugget);
+  }
+  KK_GUARD_END
+}
+
+// krige_set_grid_cv -> set_grid_cv_base (kriging_base.F90:1120-1135)
+int krige_set_grid_cv(int64_t h) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
+  e->cross_validation = 1;
+  e->bcoord = e->obs[0].coord;
+  e->nblockpnt.clear();
+  e->gcoord.clear();
+  e->gweight.clear();
+  grid_common(e, e->obs[0].n, nullptr, nullptr);
+  if (e->ndrift > 0) {
+    if (e->obs[0].drift.empty()) throw std::string("Observation drift is not set while ndrift > 0.");
+    for (int ib = 0; ib < e->nblock; ++ib)
+      for (int v = 0; v < e->nvar; ++v)
+        for (int a = 0; a < e->ndrift; ++a)
+          e->bdrift[((size_t)ib * e->nvar + v) * e->ndrift + a] = e->obs[0].drift[(size_t)ib * e->ndrift + a];
+  }
+  KK_GUARD_END
+}
+
+// krige_set_grid_drift, kriging_capi.F90:380-397 -> set_grid_drift_base (kriging_base.F90:1138-1186)
+int krige_set_grid_drift(int64_t h, int ivar, int ndrift_c, int nblocks, const double* drift) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (e->nblock == 0) throw std::string("Grid needs to be set before adding drift.");
+  if (e->ndrift == 0) throw std::string("grid/block drift is specified but ndrift==0");
+  if (ndrift_c != e->ndrift) throw std::string("size(drift, 1) /= ndrift");
+  if (nblocks != e->nblock) throw std::string("size(drift, 2) /= block%n; one drift value per block, not per grid node");
+  for (int ib = 0; ib < nblocks; ++ib)
+    for (int v = 0; v < e->nvar; ++v) {
+      if (ivar >= 1 && ivar != v + 1) continue;
+      if (ivar == 0 || ivar > e->nvar) throw std::string("ivar must be 1..nvar or < 0 (broadcast)");
+      for (int a = 0; a < ndrift_c; ++a)
+        e->bdrift[((size_t)ib * e->nvar + v) * e->ndrift + a] = drift[(size_t)ib * ndrift_c + a];
+    }
+  KK_GUARD_END
+}
+
+// krige_set_search, kriging_capi.F90:448-467 -> set_search (kriging.F90:318-387)
+int krige_set_search(int64_t h, int ivar, double anis1, double anis2, double azimuth, double dip, double plunge,
+                     int sector_search) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  ObsVar& o = e->obs[ivar - 1];
+  if (o.n == 0) throw std::string("set_obs() needs to be called before set_search().");
+  o.anis1 = anis1;
+  o.anis2 = anis2;
+  o.az = azimuth;
+  o.dip = dip;
+  o.plunge = plunge;
+  o.sector = sector_search ? 1 : 0;
+  o.search_set = true;
+  o.search_dirty = true;
+  KK_GUARD_END
+}
+
+// krige_solve, kriging_capi_common.F90:229-239 -> solve_base (kriging_base.F90:2064-2194)
+int krige_solve(int64_t h, int nthread, int ncache) {
+  (void)nthread; (void)ncache;  // CPU threading / factor-cache knobs: not used on the GPU
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_solve(*e);
+  KK_GUARD_END
+}
+
+// krige_solver_stats, kriging_capi_common.F90:113-128
+void krige_solver_stats(int64_t h, int* out) {
+  Engine* e = get(h);
+  for (int i = 0; i < 5; ++i) out[i] = e ? e->stats[i] : 0;
+}
+
+int krige_get_last_error(char* buffer, int nbuf) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  if (nbuf > 0) {
+    size_t n = std::min<size_t>(g_err.size(), (size_t)nbuf - 1);
+    std::memcpy(buffer, g_err.data(), n);
+    buffer[n] = 0;
+  }
+  return g_err.empty() ? 0 : 1;
+}
+
+int krige_get_nblocks(int64_t h, int* nb) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  *nb = e->nblock;
+  KK_GUARD_END
+}
+
+int krige_get_nsim(int64_t h, int* ns) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  *ns = 0;
+  KK_GUARD_END
+}
+
+// krige_get_block_coord, kriging_capi_common.F90:277-288
+int krige_get_block_coord(int64_t h, int ndim_c, int nblocks, double* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib)
+    for (int k = 0; k < ndim_c; ++k) out[(size_t)ib * ndim_c + k] = e->bcoord[(size_t)ib * e->nlag + k];
+  KK_GUARD_END
+}
+
+static void check_solved(Engine* e) {
+  if (!e->solved) throw std::string("solve() has not been called; call solve() before retrieving results");
+}
+
+// krige_get_estimate_all, kriging_capi_common.F90:323-344: out(nblocks, nvar, nsim)
+int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, double* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  check_solved(e);
+  const int nv = e->nvar;
+  std::vector<double> tmp((size_t)e->nblock * nv);
+  cudaMemcpy(tmp.data(), e->est.p, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost);
+  for (int is = 0; is < nsim_c; ++is)
+    for (int iv = 0; iv < nvar_c; ++iv)
+      for (int ib = 0; ib < nblocks; ++ib)
+        out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * is)] = tmp[(size_t)ib * nv + iv];
+  KK_GUARD_END
+}
+
+// krige_get_estimate, kriging_capi_common.F90:290-306: out(nblocks, nsim) of variable 1
+int krige_get_estimate(int64_t h, int nsim_c, int nblocks, double* out) {
+  return krige_get_estimate_all(h, nblocks, 1, nsim_c, out);
+}
+
+// krige_get_variance_all, kriging_capi_common.F90:372-392: out(nblocks, nvar, nvar)
+int krige_get_variance_all(int64_t h, int nblocks, int nvar_c, double* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  check_solved(e);
+  const int nv = e->nvar;
+  std::vector<double> tmp((size_t)e->nblock * nv * nv);
+  cudaMemcpy(tmp.data(), e->var.p, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost);
+  for (int jv = 0; jv < nvar_c; ++jv)
+    for (int iv = 0; iv < nvar_c; ++iv)
+      for (int ib = 0; ib < nblocks; ++ib)
+        out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * jv)] = tmp[(size_t)ib * nv * nv + iv + (size_t)jv * nv];
+  KK_GUARD_END
+}
+
+// krige_get_variance, kriging_capi_common.F90:352-369: variance of variable 1
+int krige_get_variance(int64_t h, int nblocks, double* out) {
+  return krige_get_variance_all(h, nblocks, 1, out);
+}
+
+// ---------------------------------------------------------------------------
+// extensions (no reference counterpart; see include/krigekit_b200.h)
+// ---------------------------------------------------------------------------
+int krige_set_precision(int64_t h, int mode) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (mode != 0 && mode != 1) throw std::string("precision mode must be 0 (fp64) or 1 (fp32_refine)");
+  e->precision = mode;
+  KK_GUARD_END
+}
+
+int krige_set_nmin(int64_t h, int nmin) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  e->nmin = nmin;
+  KK_GUARD_END
+}
+
+int krige_set_device(int64_t h, int device, void* stream) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  e->device = device;
+  e->stream = (cudaStream_t)stream;
+  KK_GUARD_END
+}
+
+void krige_set_allocator(void* (*alloc)(size_t, void*), void (*release)(void*, void*), void* ctx) {
+  set_allocator(alloc, release, ctx);
+}
+
+// neighbour sets after solve(): nnear(nblocks), inear(mmax, nblocks) 1-based, ascending
+int krige_get_neighbours(int64_t h, int ivar, int nblocks, int mmax, int* nnear, int* inear) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  check_solved(e);
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  VarDevice& d = e->vd[ivar - 1];
+  const int mm = std::max(d.search.mmax, 1);
+  std::vector<int> nn(e->nblock), nb((size_t)e->nblock * mm);
+  cudaMemcpy(nn.data(), d.nnear.p, sizeof(int) * nn.size(), cudaMemcpyDeviceToHost);
+  cudaMemcpy(nb.data(), d.nbr.p, sizeof(int) * nb.size(), cudaMemcpyDeviceToHost);
+  for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib) {
+    nnear[ib] = nn[ib];
+    for (int k = 0; k < mmax; ++k) inear[(size_t)ib * mmax + k] = (k < nn[ib] && k < mm) ? nb[(size_t)ib * mm + k] + 1 : 0;
+  }
+  KK_GUARD_END
+}
+
+int krige_get_mmax(int64_t h, int ivar, int* mmax) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (ivar < 1 || ivar > e->nvar) throw std::string("ivar out of range");
+  *mmax = std::max(e->vd[ivar - 1].search.mmax, 1);
+  KK_GUARD_END
+}
+
+// per-target status bits (KK_ST_* in kk_common.h)
+int krige_get_status(int64_t h, int nblocks, int* status) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  check_solved(e);
+  std::vector<int> s(e->nblock);
+  cudaMemcpy(s.data(), e->status.p, sizeof(int) * s.size(), cudaMemcpyDeviceToHost);
+  for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib) status[ib] = s[ib];
+  KK_GUARD_END
+}
+
+// counters of the last solve: [fail, chol, 0, ldlt, 0, search redo, fp64 re-solve, refine iterations]
+int krige_gpu_stats(int64_t h, int* out8, double* solve_ms) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  for (int i = 0; i < 8; ++i) out8[i] = e->stats[i];
+  if (solve_ms) *solve_ms = e->last_solve_ms;
+  KK_GUARD_END
+}
+
+}  // extern "C"

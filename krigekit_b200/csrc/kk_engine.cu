@@ -1,0 +1,496 @@
+// kk_engine.cu -- solve() orchestration on one device for one handle.
+//
+// Data flow of one solve (solve_base, kriging_base.F90:2064-2194):
+//   prepare    host: variogram tables + search parameters; device: upload of
+//              changed observations/targets, grid build per variable
+//   search     k_search per variable (+ exact kd-tree replica for targets
+//              whose selection boundary has equal distances)
+//   bucket     size buckets of npp per target
+//   solve      register kernels per bucket (FP64, or FP32 + FP64
+//              refinement), FP64 re-solve of non-converged targets, generic
+//              kernel for n > 64 and Cholesky failures (LDL^T + jitter)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kk_host.h"
+#include "kk_kernels.h"
+
+namespace kk {
+
+static alloc_fn g_alloc = nullptr;
+static free_fn g_free = nullptr;
+static void* g_actx = nullptr;
+
+void set_allocator(alloc_fn a, free_fn f, void* ctx) {
+  g_alloc = a;
+  g_free = f;
+  g_actx = ctx;
+}
+
+#define KK_CUDA(x)                                                                    \
+  do {                                                                                \
+    cudaError_t err__ = (x);                                                          \
+    if (err__ != cudaSuccess) {                                                       \
+      throw std::string("CUDA error ") + cudaGetErrorString(err__) + " at " #x;       \
+    }                                                                                 \
+  } while (0)
+
+void DBuf::reserve(size_t b) {
+  if (b <= bytes && p) return;
+  release();
+  size_t nb = b < 256 ? 256 : b;
+  if (g_alloc) {
+    p = g_alloc(nb, g_actx);
+    if (!p) throw std::string("device allocation failed (registered allocator)");
+  } else {
+    KK_CUDA(cudaMalloc(&p, nb));
+  }
+  bytes = nb;
+}
+
+void DBuf::release() {
+  if (!p) return;
+  if (g_alloc) g_free(p, g_actx);
+  else cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+static void upload(DBuf& d, const void* h, size_t bytes, cudaStream_t st) {
+  d.reserve(bytes);
+  if (bytes) KK_CUDA(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, st));
+}
+
+static int sm_count(int dev) {
+  static int cached[64] = {0};
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) cudaDeviceGetAttribute(&cached[dev], cudaDevAttrMultiProcessorCount, dev);
+  return cached[dev];
+}
+
+// search parameters for variable v (set_search, kriging.F90:318-387;
+// kriging_st.F90:322-403) and the matrix sizing (prepare_common,
+// kriging_base.F90:3003-3012)
+static void setup_search(Engine& e, int v, KkSearch& S) {
+  const ObsVar& o = e.obs[v];
+  std::memset(&S, 0, sizeof S);
+  S.ndim = e.ndim;
+  S.nlag = e.nlag;
+  S.st = e.st;
+  S.nobs = o.n;
+  S.cv = (e.cross_validation != 0);
+  int nmax = o.nmax;
+  if (e.cross_validation && v == 0 && nmax > 0 && nmax < INT_MAX) nmax = nmax + 1;  // set_grid_cv_base
+  if (nmax > o.n) nmax = o.n;
+  if (nmax <= 0) nmax = o.n;
+  const bool need = o.n > nmax;
+  const double eps = 1.0e-10;
+  S.aniso = ((std::fabs(o.anis1 - 1.0) > eps || std::fabs(o.anis2 - 1.0) > eps) && e.anisotropic_search) ? 1 : 0;
+  double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::memcpy(S.rotmat, eye, sizeof eye);
+  if (e.st || (need && S.aniso)) calc_rotmat(o.az, o.dip, o.plunge, o.anis1, o.anis2, S.rotmat);
+  S.maxd2 = o.maxdist * o.maxdist;
+  S.ta = o.time_at;
+  S.nmax = nmax;
+  if (!need) {
+    S.mode = 0;
+    S.K = o.n;
+    S.mmax = o.n;
+  } else if (o.sector) {
+    S.mode = 2;
+    long long lim = (long long)(1 << e.ndim) * nmax * 4;
+    S.K = (int)std::min<long long>(o.n, lim);
+    S.mmax = (1 << e.ndim) * nmax;
+  } else {
+    S.mode = 1;
+    S.K = nmax;
+    S.mmax = nmax;
+  }
+}
+
+// uniform grid over the search coordinates of variable v
+static void build_grid(Engine& e, int v) {
+  VarDevice& d = e.vd[v];
+  KkSearch& S = d.search;
+  const int n = S.nobs;
+  const int D = e.nlag;
+  cudaStream_t st = e.stream;
+  DBuf scu;
+  scu.reserve(sizeof(double) * (size_t)D * n);
+  const double* xs[4] = {d.x[0].as<double>(), d.x[1].as<double>(), d.x[2].as<double>(), d.x[3].as<double>()};
+  KkGrid& g = S.grid;
+  g.D = D;
+  launch_search_coords(S, xs, scu.as<double>(), n, st);
+  std::vector<double> h((size_t)D * n);
+  KK_CUDA(cudaMemcpyAsync(h.data(), scu.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < D; ++k) {
+    double lo = h[(size_t)k * n], hi = lo;
+    for (int i = 1; i < n; ++i) {
+      double x = h[(size_t)k * n + i];
+      lo = std::min(lo, x);
+      hi = std::max(hi, x);
+    }
+    g.umin[k] = lo;
+    g.umax[k] = hi;
+  }
+  g.G = std::min(D, 3);
+  g.nobs = n;
+  // cell size for about two points per cell on average
+  double ext[3], vol = 1.0, emax = 0.0;
+  for (int k = 0; k < g.G; ++k) emax = std::max(emax, g.umax[k] - g.umin[k]);
+  if (emax <= 0.0) emax = 1.0;
+  for (int k = 0; k < g.G; ++k) {
+    ext[k] = std::max(g.umax[k] - g.umin[k], 1e-9 * emax);
+    vol *= ext[k];
+  }
+  const double occ = 2.0;
+  double hcell = std::pow(vol * occ / std::max(n, 1), 1.0 / g.G);
+  long long ncell = 1;
+  for (int k = 0; k < g.G; ++k) {
+    long long c = (long long)std::ceil(ext[k] / hcell);
+    c = std::max<long long>(1, std::min<long long>(c, 1 << 14));
+    g.n[k] = (int)c;
+    ncell *= c;
+  }
+  while (ncell > (1ll << 26)) {
+    ncell = 1;
+    for (int k = 0; k < g.G; ++k) { g.n[k] = std::max(1, g.n[k] / 2); ncell *= g.n[k]; }
+  }
+  for (int k = 0; k < 3; ++k) {
+    if (k >= g.G) { g.n[k] = 1; g.lo[k] = 0; g.h[k] = 1; g.inv_h[k] = 1; continue; }
+    g.lo[k] = g.umin[k];
+    g.h[k] = ext[k] / g.n[k] * (1.0 + 1e-12);
+    g.inv_h[k] = 1.0 / g.h[k];
+  }
+  const long long nsat = (long long)(g.n[0] + 1) * (g.n[1] + 1) * (g.n[2] + 1);
+  d.cell_of.reserve(sizeof(int) * n);
+  DBuf count;
+  count.reserve(sizeof(int) * ncell);
+  d.cursor.reserve(sizeof(int) * ncell);
+  d.cell_start.reserve(sizeof(int) * (ncell + 1));
+  d.sc.reserve(sizeof(double) * (size_t)D * n);
+  d.sidx.reserve(sizeof(int) * n);
+  d.sat.reserve(sizeof(int) * nsat);
+  launch_grid_build(g, scu.as<double>(), d.cell_of.as<int>(), count.as<int>(), d.cell_start.as<int>(),
+                    d.cursor.as<int>(), d.sc.as<double>(), d.sidx.as<int>(), d.sat.as<int>(), n, st);
+  g.cell_start = d.cell_start.as<int>();
+  g.sat = d.sat.as<int>();
+  g.sc = d.sc.as<double>();
+  g.sidx = d.sidx.as<int>();
+  KK_CUDA(cudaStreamSynchronize(st));
+  // keep the search coordinates in original order for a kd-tree build on demand
+  d.tree_rdata.reserve(sizeof(double) * h.size());
+  KK_CUDA(cudaMemcpyAsync(d.tree_rdata.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+  d.grid_ready = true;
+  d.tree_ready = false;
+}
+
+// kd-tree for the exact tie fallback (kdtree2_create on the search coords)
+static void build_tree(Engine& e, int v) {
+  VarDevice& d = e.vd[v];
+  KkSearch& S = d.search;
+  const int n = S.nobs, D = e.nlag;
+  std::vector<double> soa((size_t)D * n), pm((size_t)D * n);
+  KK_CUDA(cudaMemcpyAsync(soa.data(), d.tree_rdata.p, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, e.stream));
+  KK_CUDA(cudaStreamSynchronize(e.stream));
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < D; ++k) pm[(size_t)i * D + k] = soa[(size_t)k * n + i];
+  std::vector<int> ni, ind;
+  std::vector<double> nd, box, rdata;
+  int root = 0;
+  build_kdtree(pm.data(), D, n, ni, nd, box, ind, rdata, root);
+  upload(d.tree_i, ni.data(), sizeof(int) * ni.size(), e.stream);
+  upload(d.tree_d, nd.data(), sizeof(double) * nd.size(), e.stream);
+  upload(d.tree_box, box.data(), sizeof(double) * box.size(), e.stream);
+  upload(d.tree_ind, ind.data(), sizeof(int) * ind.size(), e.stream);
+  DBuf tmp;
+  upload(tmp, rdata.data(), sizeof(double) * rdata.size(), e.stream);
+  KK_CUDA(cudaStreamSynchronize(e.stream));
+  d.tree_rdata.release();
+  std::swap(d.tree_rdata.p, tmp.p);
+  std::swap(d.tree_rdata.bytes, tmp.bytes);
+  KkTree& T = S.tree;
+  T.D = D;
+  T.n = n;
+  T.nnodes = (int)(ni.size() / 5);
+  T.root = root;
+  T.node_i = d.tree_i.as<int>();
+  T.node_d = d.tree_d.as<double>();
+  T.box = d.tree_box.as<double>();
+  T.ind = d.tree_ind.as<int>();
+  T.rdata = d.tree_rdata.as<double>();
+  d.tree_ready = true;
+}
+
+static void validate(const Engine& e) {
+  if (e.nblock <= 0) throw std::string("Call set_grid() before solve().");
+  for (int v = 0; v < e.nvar; ++v) {
+    if (e.obs[v].n == 0) throw std::string("Call set_obs() for every variable before solve().");
+    if (!e.obs[v].search_set) throw std::string("set_search() needs to be called before solve().");
+    if (e.ndrift > 0 && e.obs[v].drift.empty())
+      throw std::string("Observation drift is not set while ndrift > 0.");
+  }
+  if (e.ndrift > 0 && e.bdrift.empty()) throw std::string("Grid drift is not set while ndrift > 0.");
+  for (int a = 0; a < e.nvar; ++a)
+    for (int b = a; b < e.nvar; ++b)
+      if (e.vgm[a][b].empty()) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "variogram not set for ivar=%d, jvar=%d. Call set_vgm().", a + 1, b + 1);
+        throw std::string(msg);
+      }
+}
+
+void engine_solve(Engine& e) {
+  auto t0 = std::chrono::steady_clock::now();
+  e.solved = false;
+  std::memset(e.stats, 0, sizeof e.stats);
+  validate(e);
+  KK_CUDA(cudaSetDevice(e.device));
+  cudaStream_t st = e.stream;
+  const int nsm = sm_count(e.device);
+  set_zones(st);
+  const int nv = e.nvar, nb = e.nblock, D = e.nlag;
+
+  // ---- variogram models and tables (prepare, kriging.F90:398-424)
+  std::vector<KkModel> mdl;
+  std::vector<KkSTModel> smdl;
+  std::vector<double2> tabs;
+  build_models(e, mdl, smdl, tabs);
+  if (tabs.empty()) tabs.push_back(make_double2(0.0, 0.0));
+  upload(e.tables, tabs.data(), sizeof(double2) * tabs.size(), st);
+  if (e.st) upload(e.models, smdl.data(), sizeof(KkSTModel) * smdl.size(), st);
+  else upload(e.models, mdl.data(), sizeof(KkModel) * mdl.size(), st);
+
+  // ---- observations + search structures
+  for (int v = 0; v < nv; ++v) {
+    ObsVar& o = e.obs[v];
+    VarDevice& d = e.vd[v];
+    const int n = o.n;
+    if (o.dirty) {
+      std::vector<double> tmp(n);
+      for (int k = 0; k < D; ++k) {
+        for (int i = 0; i < n; ++i) tmp[i] = o.coord[(size_t)i * D + k];
+        upload(d.x[k], tmp.data(), sizeof(double) * n, st);
+      }
+      for (int k = D; k < 4; ++k) d.x[k].reserve(8);
+      upload(d.value, o.value.data(), sizeof(double) * n, st);
+      upload(d.variance, o.variance.data(), sizeof(double) * n, st);
+      if (e.ndrift > 0) {
+        std::vector<double> dr((size_t)e.ndrift * n);
+        for (int i = 0; i < n; ++i)
+          for (int a = 0; a < e.ndrift; ++a) dr[(size_t)a * n + i] = o.drift[(size_t)i * e.ndrift + a];
+        upload(d.drift, dr.data(), sizeof(double) * dr.size(), st);
+      } else {
+        d.drift.reserve(8);
+      }
+      KK_CUDA(cudaStreamSynchronize(st));
+    }
+    KkSearch S;
+    setup_search(e, v, S);
+    const bool rebuild = o.dirty || o.search_dirty || !d.grid_ready ||
+                         std::memcmp(S.rotmat, d.search.rotmat, sizeof S.rotmat) != 0 ||
+                         S.aniso != d.search.aniso || S.ta != d.search.ta;
+    KkGrid keep_grid = d.search.grid;
+    KkTree keep_tree = d.search.tree;
+    d.search = S;
+    if (S.mode != 0) {
+      if (rebuild) build_grid(e, v);
+      else { d.search.grid = keep_grid; d.search.tree = keep_tree; }
+    } else {
+      d.grid_ready = false;
+    }
+    o.dirty = false;
+    o.search_dirty = false;
+  }
+
+  // ---- targets
+  if (e.grid_dirty) {
+    std::vector<double> tmp(nb);
+    for (int k = 0; k < D; ++k) {
+      for (int i = 0; i < nb; ++i) tmp[i] = e.bcoord[(size_t)i * D + k];
+      upload(e.tx[k], tmp.data(), sizeof(double) * nb, st);
+    }
+    for (int k = D; k < 4; ++k) e.tx[k].reserve(8);
+    if (!e.rangescale.empty()) upload(e.trs, e.rangescale.data(), sizeof(double) * nb, st);
+    if (!e.localnugget.empty()) upload(e.tln, e.localnugget.data(), sizeof(double) * nb, st);
+    if (!e.nblockpnt.empty()) {
+      std::vector<int> gs(nb + 1, 0);
+      for (int i = 0; i < nb; ++i) gs[i + 1] = gs[i] + e.nblockpnt[i];
+      upload(e.gstart, gs.data(), sizeof(int) * gs.size(), st);
+      const int ng = gs[nb];
+      std::vector<double> gt(ng);
+      for (int k = 0; k < D; ++k) {
+        for (int i = 0; i < ng; ++i) gt[i] = e.gcoord[(size_t)i * D + k];
+        upload(e.gx[k], gt.data(), sizeof(double) * ng, st);
+      }
+      upload(e.gw, e.gweight.data(), sizeof(double) * ng, st);
+    }
+    KK_CUDA(cudaStreamSynchronize(st));
+    e.grid_dirty = false;
+  }
+  if (e.ndrift > 0) upload(e.tdrift, e.bdrift.data(), sizeof(double) * e.bdrift.size(), st);
+
+  // ---- outputs and work buffers
+  e.est.reserve(sizeof(double) * (size_t)nb * nv);
+  e.var.reserve(sizeof(double) * (size_t)nb * nv * nv);
+  e.status.reserve(sizeof(int) * nb);
+  e.counters.reserve(sizeof(int) * KK_CNT_N);
+  e.bucket.reserve(sizeof(int) * (size_t)nb * 3);
+  e.npp.reserve(sizeof(int) * (size_t)nb * 2);  // fb + fp64 lists
+  KK_CUDA(cudaMemsetAsync(e.counters.p, 0, sizeof(int) * KK_CNT_N, st));
+  KK_CUDA(cudaMemsetAsync(e.status.p, 0, sizeof(int) * nb, st));
+  int* redo = e.npp.as<int>();  // reuse the fallback list storage for search redo lists
+
+  // ---- neighbour search per variable
+  int mm_total = 0;
+  for (int v = 0; v < nv; ++v) {
+    VarDevice& d = e.vd[v];
+    KkSearch& S = d.search;
+    d.nbr.reserve(sizeof(int) * (size_t)nb * std::max(S.mmax, 1));
+    d.nnear.reserve(sizeof(int) * nb);
+    mm_total += S.mmax;
+    const double* tx[4] = {e.tx[0].as<double>(), e.tx[1].as<double>(), e.tx[2].as<double>(), e.tx[3].as<double>()};
+    const double* ox[4] = {d.x[0].as<double>(), d.x[1].as<double>(), d.x[2].as<double>(), d.x[3].as<double>()};
+    KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + KK_CNT_REDO + v, 0, sizeof(int), st));
+    launch_search(S, nb, tx, ox, d.nbr.as<int>(), d.nnear.as<int>(), e.status.as<int>(), redo,
+                  e.counters.as<int>() + KK_CNT_REDO + v, nsm, st);
+    KK_CUDA(cudaGetLastError());
+    int nredo = 0;
+    KK_CUDA(cudaMemcpyAsync(&nredo, e.counters.as<int>() + KK_CNT_REDO + v, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    e.stats[5] += nredo;
+    if (nredo > 0) {
+      if (!d.tree_ready) build_tree(e, v);
+      const int nthreads = std::min(nredo, 8192);
+      const int stride = S.K + 2;
+      DBuf heaps;
+      heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);
+      launch_search_kdtree(S, redo, e.counters.as<int>() + KK_CNT_REDO + v, tx, ox, d.nbr.as<int>(),
+                           d.nnear.as<int>(), e.status.as<int>(), heaps.p, stride, nthreads, st);
+      KK_CUDA(cudaGetLastError());
+      KK_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  e.mmax_total = mm_total;
+
+  // ---- solve parameters
+  SolveParams P;
+  std::memset(&P, 0, sizeof P);
+  P.nvar = nv;
+  P.ndim = e.ndim;
+  P.nlag = e.nlag;
+  P.st = e.st;
+  P.ndrift = e.ndrift;
+  P.naug = e.naug();
+  P.pa = e.pdrift();
+  P.std_ck = e.std_ck;
+  P.unbias = e.unbias;
+  P.ck_isa = (!e.std_ck && e.unbias != 0 && nv > 1) ? 1 : 0;
+  P.sk_any = 0;
+  for (int v = 0; v < nv; ++v) {
+    P.sk_mean[v] = e.obs[v].sk_mean;
+    if (e.unbias == 0 && e.obs[v].sk_mean != 0.0) P.sk_any = 1;
+  }
+  P.nmin = e.nmin;
+  P.neglect_error = e.neglect_error;
+  P.bounds[0] = e.bounds[0];
+  P.bounds[1] = e.bounds[1];
+  P.models = e.st ? nullptr : e.models.as<KkModel>();
+  P.smodels = e.st ? e.models.as<KkSTModel>() : nullptr;
+  P.tables = e.tables.as<double2>();
+  for (int v = 0; v < nv; ++v) {
+    VarDevice& d = e.vd[v];
+    for (int k = 0; k < 4; ++k) P.ox[v][k] = d.x[k].as<double>();
+    P.oval[v] = d.value.as<double>();
+    P.ovar[v] = d.variance.as<double>();
+    P.odrift[v] = d.drift.as<double>();
+    P.nobs[v] = e.obs[v].n;
+    P.nbr[v] = d.nbr.as<int>();
+    P.nnear[v] = d.nnear.as<int>();
+    P.mmax[v] = std::max(d.search.mmax, 1);
+  }
+  P.nblock = nb;
+  for (int k = 0; k < 4; ++k) P.tx[k] = e.tx[k].as<double>();
+  P.rs = e.rangescale.empty() ? nullptr : e.trs.as<double>();
+  P.ln = e.localnugget.empty() ? nullptr : e.tln.as<double>();
+  P.tdrift = e.ndrift > 0 ? e.tdrift.as<double>() : nullptr;
+  P.gstart = e.nblockpnt.empty() ? nullptr : e.gstart.as<int>();
+  for (int k = 0; k < 4; ++k) P.gx[k] = e.nblockpnt.empty() ? nullptr : e.gx[k].as<double>();
+  P.gw = e.nblockpnt.empty() ? nullptr : e.gw.as<double>();
+  P.est = e.est.as<double>();
+  P.var = e.var.as<double>();
+  P.status = e.status.as<int>();
+  P.counters = e.counters.as<int>();
+  P.fb_list = e.npp.as<int>();
+  P.fp64_list = e.npp.as<int>() + nb;
+  P.refine_tol = 1.0e-10;
+  if (P.pa + nv + 1 + ((P.ck_isa || P.sk_any) ? nv : 0) > 8)
+    throw std::string("too many drift/variable columns for the register kernels (max 8)");
+
+  // ---- bucket + solve
+  launch_bucket(P, e.bucket.as<int>(), st);
+  launch_solve(P, e.precision, e.bucket.as<int>(), nsm, st);
+  KK_CUDA(cudaGetLastError());
+  if (e.precision != 0) {
+    // FP32 targets whose refinement did not converge: FP64 register kernel
+    launch_solve_fp64_list(P, P.fp64_list, KK_CNT_FP64, nsm, st);
+    KK_CUDA(cudaGetLastError());
+  }
+  int cnt[KK_CNT_N];
+  KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaStreamSynchronize(st));
+  // generic path: n > 64 bucket and Cholesky failures
+  const int nbig = cnt[KK_CNT_BIG], nfb = cnt[KK_CNT_FB];
+  if (nbig > 0 || nfb > 0) {
+    int mtot = mm_total + P.pa;
+    size_t stride = (size_t)mtot * mtot * 2 + (size_t)nv * mtot * 3 + (size_t)mtot * (P.pa + 2) +
+                    (size_t)(P.pa + 1) * (P.pa + 1) + (size_t)(P.pa + 1) * nv + (size_t)mtot + 64;
+    const int nthreads = std::max(1, std::min(std::max(nbig, nfb), 2048));
+    e.scratch.reserve(sizeof(double) * stride * nthreads);
+    P.scratch = e.scratch.as<double>();
+    P.scratch_stride = (int)stride;
+    if (nbig > 0)
+      launch_solve_generic(P, e.bucket.as<int>() + (size_t)KK_CNT_BIG * nb, KK_CNT_BIG, std::min(nbig, 2048), st);
+    if (nfb > 0) launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(nfb, 2048), st);
+    KK_CUDA(cudaGetLastError());
+    KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+  }
+  // solver_stats: fail, chol_fact, chol_reuse, ssytrf_fact, ssytrf_reuse
+  e.stats[0] = cnt[KK_CNT_FAIL];
+  e.stats[1] = cnt[KK_CNT_CHOL];
+  e.stats[2] = 0;
+  e.stats[3] = cnt[KK_CNT_LDLT];
+  e.stats[4] = 0;
+  e.stats[6] = cnt[KK_CNT_FP64];
+  e.stats[7] = cnt[KK_CNT_ITER];
+  if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");
+  e.solved = true;
+  e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void engine_release(Engine& e) {
+  for (int v = 0; v < KK_MAXVAR; ++v) {
+    VarDevice& d = e.vd[v];
+    for (auto& b : d.x) b.release();
+    d.value.release(); d.variance.release(); d.drift.release();
+    d.sc.release(); d.sidx.release(); d.cell_start.release(); d.sat.release(); d.cell_of.release();
+    d.cursor.release(); d.tree_i.release(); d.tree_d.release(); d.tree_box.release(); d.tree_ind.release();
+    d.tree_rdata.release(); d.nbr.release(); d.nnear.release();
+  }
+  e.models.release(); e.tables.release();
+  for (auto& b : e.tx) b.release();
+  for (auto& b : e.gx) b.release();
+  e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
+  e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
+  e.counters.release(); e.scratch.release();
+}
+
+}  // namespace kk

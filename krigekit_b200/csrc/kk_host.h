@@ -1,0 +1,127 @@
+// kk_host.h -- host-side engine state behind the krige_* C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cfloat>
+#include <string>
+#include <vector>
+
+#include "kk_common.h"
+
+namespace kk {
+
+struct StructSpec {
+  int vtype = KK_SPH;
+  double nugget = 0.0, sill = 1.0;
+  double a_major = 1.0, a_minor1 = 1.0, a_minor2 = 1.0;
+  double az = 0.0, dip = 0.0, plunge = 0.0;
+  int is_product = 0;
+};
+
+struct ObsVar {
+  int n = 0;
+  std::vector<double> coord;     // (nlag, n) column-major, as passed to krige_set_obs
+  std::vector<double> value, variance, drift;  // drift: (ndrift, n)
+  int nmax = INT_MAX;
+  double maxdist = DBL_MAX;
+  double sk_mean = 0.0;
+  bool search_set = false;
+  double anis1 = 1.0, anis2 = 1.0, az = 0.0, dip = 0.0, plunge = 0.0, time_at = 1.0;
+  int sector = 0;
+  bool dirty = true;             // observation data changed since the last upload
+  bool search_dirty = true;      // search parameters changed since the last grid build
+};
+
+// device buffer owned through the engine allocator
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t b);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+  ~DBuf() { release(); }
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+};
+
+struct VarDevice {
+  DBuf x[4];          // observation coordinates SoA (nlag)
+  DBuf value, variance, drift;  // drift SoA: (ndrift) x n
+  DBuf sc, sidx, cell_start, sat, cell_of, cursor;
+  DBuf tree_i, tree_d, tree_box, tree_ind, tree_rdata;
+  DBuf nbr;           // (nblock, mmax) sorted neighbour indices
+  DBuf nnear;         // (nblock)
+  KkSearch search{};
+  bool grid_ready = false;
+  bool tree_ready = false;
+  long long tree_n = 0;
+};
+
+struct Engine {
+  // options (krige_initialize, kriging_base.F90:467-553)
+  int ndim = 2, nlag = 2, nvar = 1, ndrift = 0, unbias = 1, nsim = 0;
+  int anisotropic_search = 0, neglect_error = 1, std_ck = 0, cross_validation = 0;
+  int verbose = 0;
+  double bounds[2] = {-DBL_MAX, DBL_MAX};
+  int st = 0;
+  int precision = 1;   // 0 = FP64 plain, 1 = FP32 factor + FP64 refinement
+  int nmin = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+
+  std::vector<ObsVar> obs;
+  std::vector<StructSpec> vgm[KK_MAXVAR][KK_MAXVAR];
+  // space-time model (kriging_st.F90)
+  int st_model = 0, st_transform = KK_LIN;
+  double st_at = 1.0, st_k_ps = 0.0, st_time_nugget = 0.0, st_time_sill = 1.0;
+  std::vector<StructSpec> vgm_t[KK_MAXVAR][KK_MAXVAR];
+  std::vector<double> joint[KK_MAXVAR][KK_MAXVAR];
+
+  // targets
+  int nblock = 0;
+  std::vector<double> bcoord;       // (nlag, nblock)
+  std::vector<int> nblockpnt;       // empty -> point targets
+  std::vector<double> gcoord, gweight;
+  std::vector<double> rangescale, localnugget;
+  std::vector<double> bdrift;       // (ndrift, nvar, nblock)
+  bool grid_dirty = true;
+
+  // device state
+  VarDevice vd[KK_MAXVAR];
+  DBuf models, tables, tx[4], trs, tln, tdrift, gstart, gx[4], gw;
+  DBuf est, var, status, npp, bucket, counters, scratch;
+  size_t scratch_bytes = 0;
+  int mmax_total = 0;
+  bool solved = false;
+  int stats[8] = {0};
+  double last_solve_ms = 0.0;
+
+  int naug() const { return std_ck ? unbias * nvar : unbias; }
+  int pdrift() const { return ndrift + naug(); }
+};
+
+// host-side model building (kk_host.cpp)
+void calc_rotmat(double ang1, double ang2, double ang3, double anis1, double anis2, double* m);
+void build_models(const Engine& e, std::vector<KkModel>& mdl, std::vector<KkSTModel>& smdl,
+                  std::vector<double2>& tables);
+void build_kdtree(const double* data, int D, int n, std::vector<int>& node_i,
+                  std::vector<double>& node_d, std::vector<double>& box, std::vector<int>& ind,
+                  std::vector<double>& rdata, int& root);
+
+// engine entry points (kk_engine.cu)
+void engine_solve(Engine& e);
+void engine_release(Engine& e);
+
+// allocator hook
+typedef void* (*alloc_fn)(size_t bytes, void* ctx);
+typedef void (*free_fn)(void* ptr, void* ctx);
+void set_allocator(alloc_fn a, free_fn f, void* ctx);
+
+// error slot (kriging_err.f90): first error since the last clear
+void set_error(const std::string& msg);
+void clear_error();
+bool failed();
+
+}  // namespace kk

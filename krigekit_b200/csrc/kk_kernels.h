@@ -1,0 +1,84 @@
+// kk_kernels.h -- launchers of the sm_100a kernels (kk_search.cu, kk_solve.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "kk_common.h"
+
+namespace kk {
+
+// Everything the solve kernels read for one solve() call.
+struct SolveParams {
+  int nvar, ndim, nlag, st;
+  int ndrift, pa, naug, std_ck, unbias;
+  int ck_isa;        // Isaaks & Srivastava mean correction (estimate_block_base)
+  int sk_any;        // simple kriging with a non-zero mean
+  int nmin;
+  int neglect_error;
+  double bounds[2];
+  double sk_mean[KK_MAXVAR];
+  const KkModel* models;     // nvar * nvar, [first * nvar + second]
+  const KkSTModel* smodels;  // space-time models or null
+  const double2* tables;
+  // observations per variable (SoA)
+  const double* ox[KK_MAXVAR][4];
+  const double* oval[KK_MAXVAR];
+  const double* ovar[KK_MAXVAR];
+  const double* odrift[KK_MAXVAR];  // (ndrift) x nobs SoA
+  int nobs[KK_MAXVAR];
+  // neighbour lists
+  const int* nbr[KK_MAXVAR];
+  const int* nnear[KK_MAXVAR];
+  int mmax[KK_MAXVAR];
+  // targets
+  int nblock;
+  const double* tx[4];
+  const double* rs;          // rangescale or null
+  const double* ln;          // localnugget or null
+  const double* tdrift;      // (ndrift, nvar, nblock) or null
+  const int* gstart;         // block node CSR (nblock + 1) or null
+  const double* gx[4];
+  const double* gw;
+  // outputs
+  double* est;               // (nblock, nvar)
+  double* var;               // (nblock, nvar, nvar)
+  int* status;
+  int* counters;             // see KK_CNT_*
+  int* fb_list;              // targets needing the generic FP64 / LDL^T path
+  int* fp64_list;            // FP32 targets that need the FP64 register kernel
+  double* scratch;           // generic-path workspace
+  int scratch_stride;        // doubles per generic-path thread
+  double refine_tol;
+};
+
+enum {
+  KK_CNT_B16 = 0,   // bucket sizes (targets with npp in 2..32)
+  KK_CNT_B64 = 1,   // npp in 33..64
+  KK_CNT_BIG = 2,   // npp > 64
+  KK_CNT_FB = 3,    // generic fallback list length
+  KK_CNT_FP64 = 4,  // FP32 targets re-solved in FP64
+  KK_CNT_FAIL = 5,
+  KK_CNT_CHOL = 6,
+  KK_CNT_LDLT = 7,
+  KK_CNT_WORK0 = 8,  // persistent-kernel work counters (8..15)
+  KK_CNT_REDO = 16,  // search tie/overflow count per variable (16..19)
+  KK_CNT_ITER = 20,  // total refinement iterations
+  KK_CNT_N = 32
+};
+
+void launch_search_coords(const KkSearch& S, const double* const* x, double* scu, int n, cudaStream_t st);
+void launch_grid_build(const KkGrid& g, const double* scu, int* cell_of, int* count, int* start, int* cursor,
+                       double* sc, int* sidx, int* sat, int n, cudaStream_t st);
+void launch_search(const KkSearch& S, int ntarget, const double* const* tx, const double* const* ox, int* nbr,
+                   int* nnear, int* status, int* redo_list, int* redo_count, int nsm, cudaStream_t st);
+void launch_search_kdtree(const KkSearch& S, const int* list, const int* count, const double* const* tx,
+                          const double* const* ox, int* nbr, int* nnear, int* status, void* heaps,
+                          int heap_stride, int nthreads, cudaStream_t st);
+size_t kd_heap_entry_bytes();
+
+void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
+void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm, cudaStream_t st);
+void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_slot, int nsm, cudaStream_t st);
+void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st);
+void set_zones(cudaStream_t st);
+
+}  // namespace kk

@@ -1,0 +1,1022 @@
+// kk_solve.cu -- fused covariance assembly + factorisation + solve kernels.
+//
+// Per target the reference (kriging_base.F90:3159-3503, kriging.F90:714-1028,
+// solver.f90:224-300) assembles K (covariances between neighbours, table
+// lookup per pair), F (drift / unbiasedness rows) and the right-hand sides
+// k (covariance to the target, averaged over block nodes) and g, factors K
+// by Cholesky, forms the Schur complement S = F^T K^-1 F, and returns the
+// estimate sum z_i w_i and the conditional variance.
+//
+// Kernels here:
+//   k_bucket          npp per target -> size-bucket work lists
+//   k_solve_reg<..>   one CTA per target, thread i owns row i of K in
+//                     registers; right-looking Cholesky with one barrier per
+//                     column; right-hand sides forward-substituted in the
+//                     same sweep.  FP64: outputs from inner products of the
+//                     forward-substituted columns.  FP32: FP32 factor, FP64
+//                     refinement with K64 kept in shared memory.
+//   k_solve_generic   one thread per target in global workspace: n > 64,
+//                     Cholesky failures (Bunch-Kaufman LDL^T + jitter retry).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "kk_device.cuh"
+#include "kk_kernels.h"
+
+namespace kk {
+
+void set_zones(cudaStream_t st) {
+  KkZones z;
+  const double hb[4] = {0.0, 0.1, 0.5, 3.5};
+  const double dh[3] = {1e-5, 1e-4, 1e-3};
+  int o = 0;
+  for (int k = 0; k < 3; ++k) {
+    int n = (int)llround((hb[k + 1] - hb[k]) / dh[k]);
+    if (n < 1) n = 1;
+    z.zn[k] = n;
+    z.off[k] = o;
+    z.inv_dh[k] = (double)n / (hb[k + 1] - hb[k]);
+    o += n;
+  }
+  for (int k = 0; k < 4; ++k) z.zb[k] = hb[k];
+  cudaMemcpyToSymbolAsync(c_zones, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
+}
+
+__device__ __forceinline__ double cov_pair(const SolveParams& P, int first, int second, const double* lag) {
+  if (P.st) return st_cov(P.smodels[first * P.nvar + second], P.ndim, P.tables, lag);
+  return model_cov(P.models[first * P.nvar + second], P.tables, lag);
+}
+__device__ __forceinline__ double cov0_pair(const SolveParams& P, int first, int second) {
+  if (P.st) return P.smodels[first * P.nvar + second].cov0;
+  return P.models[first * P.nvar + second].cov0;
+}
+
+// lag = (a - b) / rangescale for spatial kriging (kriging.F90:783, 905);
+// space-time lags are not scaled (kriging_st.F90:806)
+__device__ __forceinline__ void make_lag(const SolveParams& P, const double* a, const double* b, double rs,
+                                         double* lag) {
+  for (int d = 0; d < P.nlag; ++d) {
+    double t = dsub(a[d], b[d]);
+    lag[d] = P.st ? t : t / rs;
+  }
+}
+
+// F row entry a of a neighbour of variable v at observation o (obs%drift,
+// kriging_base.F90:614-624)
+__device__ __forceinline__ double f_entry(const SolveParams& P, int a, int v, int o) {
+  if (a < P.ndrift) return __ldg(&P.odrift[v][(size_t)a * P.nobs[v] + o]);
+  int ua = a - P.ndrift;
+  return P.std_ck ? (ua == v ? 1.0 : 0.0) : (ua == 0 ? 1.0 : 0.0);
+}
+// g entry a for target variable iv (block%drift, kriging_base.F90:938-951)
+__device__ __forceinline__ double g_entry(const SolveParams& P, int a, int iv, int t) {
+  if (a < P.ndrift) return P.tdrift ? __ldg(&P.tdrift[((size_t)t * P.nvar + iv) * P.ndrift + a]) : 0.0;
+  int ua = a - P.ndrift;
+  return P.std_ck ? (ua == iv ? 1.0 : 0.0) : (ua == 0 ? 1.0 : 0.0);
+}
+
+__device__ __forceinline__ void write_nan(const SolveParams& P, int t) {
+  for (int v = 0; v < P.nvar; ++v) P.est[(size_t)t * P.nvar + v] = __longlong_as_double(0x7ff8000000000000ll);
+  for (int q = 0; q < P.nvar * P.nvar; ++q)
+    P.var[(size_t)t * P.nvar * P.nvar + q] = __longlong_as_double(0x7ff8000000000000ll);
+}
+
+// ---------------------------------------------------------------------------
+// bucketing
+// ---------------------------------------------------------------------------
+__global__ void k_bucket(SolveParams P, int* __restrict__ lists) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.nblock) return;
+  int npp = 0;
+  for (int v = 0; v < P.nvar; ++v) npp += P.nnear[v][t];
+  int slot;
+  if (npp == 0 || npp == 1 || (P.nmin > 0 && npp < P.nmin)) {
+    // zero neighbours (kriging_base.F90:3198-3207); npp == 1 reuses a stale
+    // solution in the reference and is reported as NaN here
+    write_nan(P, t);
+    P.status[t] |= KK_ST_EMPTY;
+    if (npp == 0 && !P.neglect_error) atomicAdd(&P.counters[KK_CNT_FAIL], 1);
+    return;
+  }
+  slot = npp <= 32 ? KK_CNT_B16 : (npp <= 64 ? KK_CNT_B64 : KK_CNT_BIG);
+  int p = atomicAdd(&P.counters[slot], 1);
+  lists[(size_t)slot * P.nblock + p] = t;
+}
+
+void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st) {
+  k_bucket<<<(P.nblock + 255) / 256, 256, 0, st>>>(P, lists);
+}
+
+// ---------------------------------------------------------------------------
+// shared per-target preparation (gather + RHS) used by the register kernels
+// ---------------------------------------------------------------------------
+template <int NPAD>
+struct TargetSmem {
+  int obs[NPAD];
+  int var[NPAD];
+  double x[4][NPAD];
+  double z[NPAD];
+  int t, npp, nn[KK_MAXVAR], ist[KK_MAXVAR];
+  double rs, ln;
+};
+
+constexpr int MAXC = 8;  // forward-substituted columns: F + k + functionals (z, indicators)
+
+// number of functional columns carried for the estimate
+__device__ __forceinline__ int n_func(const SolveParams& P) {
+  return 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
+}
+
+// value of functional column u at row r: z, then indicators of each variable
+template <int NPAD>
+__device__ __forceinline__ double u_entry(const TargetSmem<NPAD>& ts, int u, int r) {
+  if (u == 0) return ts.z[r];
+  return ts.var[r] == u - 1 ? 1.0 : 0.0;
+}
+
+// named barrier over the NT threads of this CTA
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if (NT <= 32) __syncwarp();
+  else __syncthreads();
+}
+
+// Covariance of neighbour row r with the target (averaged over block nodes)
+// for target variable iv (assemble_rhs, kriging.F90:889-910).
+template <int NPAD>
+__device__ double rhs_cov(const SolveParams& P, const TargetSmem<NPAD>& ts, int r, int iv) {
+  double xr[4];
+  for (int d = 0; d < P.nlag; ++d) xr[d] = ts.x[d][r];
+  const int t = ts.t;
+  double tmp = 0.0;
+  if (P.gstart) {
+    const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
+    for (int k = k0; k < k1; ++k) {
+      double node[4], lag[4];
+      for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
+      make_lag(P, xr, node, ts.rs, lag);
+      tmp = dadd(tmp, dmul(cov_pair(P, ts.var[r], iv, lag), __ldg(&P.gw[k])));
+    }
+  } else {
+    double node[4], lag[4];
+    for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
+    make_lag(P, xr, node, ts.rs, lag);
+    tmp = dadd(tmp, dmul(cov_pair(P, ts.var[r], iv, lag), 1.0));
+  }
+  return tmp;
+}
+
+// prior covariance C_ij(x0, x0) for the variance (calc_variance,
+// kriging.F90:989-1008): cov0 for points, node-pair sum for blocks.
+__device__ double base_cov(const SolveParams& P, int t, int iv, int jv) {
+  if (!P.gstart) return cov0_pair(P, iv, jv);
+  const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
+  if (k1 - k0 == 1) return cov0_pair(P, iv, jv);
+  const double c0 = cov0_pair(P, iv, jv);
+  double base = 0.0;
+  for (int i = k0; i < k1; ++i) {
+    double wi = __ldg(&P.gw[i]);
+    base = dadd(base, dmul(dmul(c0, wi), wi));
+    for (int j = i + 1; j < k1; ++j) {
+      double lag[4];
+      for (int d = 0; d < P.nlag; ++d) lag[d] = dsub(__ldg(&P.gx[d][i]), __ldg(&P.gx[d][j]));
+      base = dadd(base, dmul(dmul(dmul(cov_pair(P, iv, jv, lag), wi), __ldg(&P.gw[j])), 2.0));
+    }
+  }
+  return base;
+}
+
+// Solve the small p x p Schur system and produce est / var from the inner
+// products G (FP64).  Column order: F (pa), k (nvar), u (nu).
+// G is symmetric, stored full C x C.
+__device__ void finish_outputs(const SolveParams& P, int t, const double* G, int C, const double* zmean,
+                               int* fail) {
+  const int pa = P.pa, q = P.nvar, nu = n_func(P);
+  const int kF = 0, kK = pa, kU = pa + q;
+  double S[36], lam[KK_MAXVAR][6];
+  // S = F^T K^-1 F, Cholesky (SPOTRF 'U' semantics on p x p)
+  for (int a = 0; a < pa; ++a)
+    for (int b = 0; b < pa; ++b) S[a * 6 + b] = G[(kF + a) * C + kF + b];
+  for (int j = 0; j < pa; ++j) {
+    double ajj = S[j * 6 + j];
+    for (int k = 0; k < j; ++k) ajj -= S[k * 6 + j] * S[k * 6 + j];
+    if (!(ajj > 0.0)) { *fail = 1; return; }
+    ajj = sqrt(ajj);
+    S[j * 6 + j] = ajj;
+    for (int i = j + 1; i < pa; ++i) {
+      double s = S[j * 6 + i];
+      for (int k = 0; k < j; ++k) s -= S[k * 6 + j] * S[k * 6 + i];
+      S[j * 6 + i] = s / ajj;
+    }
+  }
+  for (int iv = 0; iv < q; ++iv) {
+    // rhs_small = F^T K^-1 k - g  (solver.f90:282-286)
+    double r[6];
+    for (int a = 0; a < pa; ++a) r[a] = G[(kF + a) * C + kK + iv] - g_entry(P, a, iv, t);
+    for (int i = 0; i < pa; ++i) {  // U^T y = r
+      double s = r[i];
+      for (int k = 0; k < i; ++k) s -= S[k * 6 + i] * r[k];
+      r[i] = s / S[i * 6 + i];
+    }
+    for (int i = pa - 1; i >= 0; --i) {  // U x = y
+      double s = r[i];
+      for (int k = i + 1; k < pa; ++k) s -= S[i * 6 + k] * r[k];
+      r[i] = s / S[i * 6 + i];
+    }
+    for (int a = 0; a < pa; ++a) lam[iv][a] = r[a];
+  }
+  // estimate (estimate_block_base, kriging_base.F90:3424-3468)
+  for (int jv = 0; jv < q; ++jv) {
+    // z^T w = z^T K^-1 k - (z^T K^-1 F) lambda
+    double avg = G[kU * C + kK + jv];
+    for (int a = 0; a < pa; ++a) avg -= G[kU * C + kF + a] * lam[jv][a];
+    if (nu > 1) {
+      double tw[KK_MAXVAR], tws = 0.0;
+      for (int v = 0; v < q; ++v) {
+        tw[v] = G[(kU + 1 + v) * C + kK + jv];
+        for (int a = 0; a < pa; ++a) tw[v] -= G[(kU + 1 + v) * C + kF + a] * lam[jv][a];
+        tws += tw[v];
+      }
+      if (P.ck_isa)
+        for (int v = 0; v < q; ++v)
+          if (v != jv && zmean[KK_MAXVAR + v] > 0.0) avg += (zmean[jv] - zmean[v]) * tw[v];
+      if (P.unbias == 0 && P.sk_mean[jv] != 0.0) avg += (1.0 - tws) * P.sk_mean[jv];
+    }
+    if (avg < P.bounds[0]) avg = P.bounds[0];
+    if (avg > P.bounds[1]) avg = P.bounds[1];
+    P.est[(size_t)t * q + jv] = avg;
+  }
+  // variance: base - (w_iv^T k_jv + lambda_iv^T g_jv) (calc_variance)
+  double* V = P.var + (size_t)t * q * q;
+  for (int iv = 0; iv < q; ++iv)
+    for (int jv = iv; jv < q; ++jv) {
+      double d = G[(kK + iv) * C + kK + jv];
+      for (int a = 0; a < pa; ++a) d -= lam[iv][a] * G[(kF + a) * C + kK + jv];
+      for (int a = 0; a < pa; ++a) d += lam[iv][a] * g_entry(P, a, jv, t);
+      double v = base_cov(P, t, iv, jv) - d;
+      V[iv + jv * q] = v;
+      V[jv + iv * q] = v;
+    }
+  for (int iv = 0; iv < q; ++iv) {
+    double d = V[iv + iv * q];
+    if (d < 0.0) V[iv + iv * q] = 0.0;
+    for (int jv = iv + 1; jv < q; ++jv) {
+      double o = V[jv + iv * q];
+      if (o < 0.0) o = 0.0;
+      V[jv + iv * q] = o;
+      V[iv + jv * q] = o;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// register kernel: one CTA of NPAD threads per target, thread i owns row i
+// ---------------------------------------------------------------------------
+template <typename T, int NPAD, bool REFINE>
+__global__ void __launch_bounds__(NPAD, 1) k_solve_reg(SolveParams P, const int* __restrict__ list,
+                                                     const int* __restrict__ list_count, int work_slot) {
+  constexpr int NT = NPAD;
+  constexpr int NK = NPAD * (NPAD + 1) / 2;
+  __shared__ TargetSmem<NPAD> ts;
+  __shared__ double Kp[NK];                 // K64 packed lower (row-major)
+  __shared__ T cb[2][NPAD + MAXC + 2];      // column broadcast (double-buffered)
+  __shared__ double cols[MAXC][NPAD];       // forward-substituted columns / W
+  __shared__ double wvec[REFINE ? MAXC : 1][NPAD];  // raw F | k | u columns (refinement)
+  __shared__ double G[MAXC * MAXC];
+  __shared__ double zmean[2 * KK_MAXVAR];
+  __shared__ int s_item, s_flag;
+  __shared__ float Ls[REFINE ? NK : 1];     // FP32 factor (packed lower) for backward sweeps
+  __shared__ double red[2][NPAD / 32 + 1];
+
+  const int i = threadIdx.x;
+  const int n_items = *list_count;
+  const int nu = n_func(P);
+  const int C = P.pa + P.nvar + nu;
+
+  for (;;) {
+    if (i == 0) s_item = atomicAdd(&P.counters[work_slot], 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= n_items) break;
+    const int t = list[item];
+    // ---- gather neighbour rows (matrix order: variable blocks, ascending index)
+    if (i == 0) {
+      int acc = 0;
+      ts.t = t;
+      for (int v = 0; v < P.nvar; ++v) {
+        ts.nn[v] = P.nnear[v][t];
+        ts.ist[v] = acc;
+        acc += ts.nn[v];
+      }
+      ts.npp = acc;
+      ts.rs = P.rs ? P.rs[t] : 1.0;
+      ts.ln = P.ln ? P.ln[t] : 0.0;
+    }
+    __syncthreads();
+    const int npp = ts.npp;
+    if (i < npp) {
+      int v = 0;
+      while (v + 1 < P.nvar && i >= ts.ist[v + 1]) ++v;
+      int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (i - ts.ist[v])]);
+      ts.obs[i] = o;
+      ts.var[i] = v;
+      for (int d = 0; d < P.nlag; ++d) ts.x[d][i] = __ldg(&P.ox[v][d][o]);
+      ts.z[i] = __ldg(&P.oval[v][o]);
+    }
+    __syncthreads();
+    // ---- assemble K (assemble_lhs, kriging.F90:714-849): pairs balanced over threads
+    const int npairs = npp * (npp - 1) / 2;
+    for (int e = i; e < npairs; e += NT) {
+      int r = (int)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+      while (r * (r - 1) / 2 > e) --r;
+      while ((r + 1) * r / 2 <= e) ++r;
+      int c = e - r * (r - 1) / 2;
+      double xc[4], xr[4], lag[4];
+      for (int d = 0; d < P.nlag; ++d) { xc[d] = ts.x[d][c]; xr[d] = ts.x[d][r]; }
+      make_lag(P, xc, xr, ts.rs, lag);
+      Kp[r * (r + 1) / 2 + c] = cov_pair(P, ts.var[r], ts.var[c], lag);
+    }
+    if (i < npp) {
+      const int v = ts.var[i];
+      double ov = __ldg(&P.ovar[v][ts.obs[i]]);
+      Kp[i * (i + 1) / 2 + i] = dadd(dadd(cov0_pair(P, v, v), ov), ts.ln);
+    }
+    // ---- right-hand-side columns for row i: F (pa), k (nvar), u (nu)
+    double b[MAXC];
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) b[c] = 0.0;
+    if (i < npp) {
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        if (c < P.pa) b[c] = f_entry(P, c, ts.var[i], ts.obs[i]);
+        else if (c < P.pa + P.nvar) b[c] = rhs_cov(P, ts, i, c - P.pa);
+        else if (!REFINE && c < C) b[c] = u_entry(ts, c - P.pa - P.nvar, i);
+      }
+    }
+    if (i == 0 && P.ck_isa) {
+      for (int v = 0; v < P.nvar; ++v) {
+        double s = 0.0;
+        for (int k = 0; k < ts.nn[v]; ++k) s = dadd(s, ts.z[ts.ist[v] + k]);
+        zmean[v] = ts.nn[v] > 0 ? s / ts.nn[v] : 0.0;
+        zmean[KK_MAXVAR + v] = (double)ts.nn[v];
+      }
+    }
+    __syncthreads();
+    // ---- load row i into registers (padding rows are identity)
+    T R[NPAD];
+#pragma unroll
+    for (int c = 0; c < NPAD; ++c) {
+      double v = 0.0;
+      if (i < npp) { if (c <= i) v = Kp[i * (i + 1) / 2 + c]; }
+      else if (c == i) v = 1.0;
+      R[c] = (T)v;
+    }
+    const int ncol = REFINE ? (P.pa + P.nvar) : C;
+    T y[MAXC];
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) y[c] = (T)b[c];
+    // warp-uniform bound on the row index of this warp
+    const int wmax = (i | 31) < npp - 1 ? (i | 31) : npp - 1;
+    if (i == 0) s_flag = 0;
+    // ---- right-looking Cholesky + forward substitution, one barrier per column
+#pragma unroll
+    for (int j = 0; j < NPAD; ++j) {
+      if (j >= npp) break;
+      T* cbj = cb[j & 1];
+      if (i >= j && i < npp) cbj[i] = R[j];
+      if (i == j) {
+        T d = R[j];
+        T inv;
+        if (!(d > (T)0)) { inv = (T)0; s_flag = 1; }
+        else inv = (T)1 / sqrt(d);
+        cbj[NPAD + MAXC] = inv;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < ncol) cbj[NPAD + c] = y[c];
+      }
+      __syncthreads();
+      if (s_flag) break;
+      const T inv = cbj[NPAD + MAXC];
+      if (i == j) {
+        R[j] = R[j] * inv;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < ncol) y[c] = y[c] * inv;
+      } else if (i > j && i < npp) {
+        const T li = R[j] * inv;
+        const T tt = li * inv;
+        R[j] = li;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < ncol) y[c] = y[c] - li * (cbj[NPAD + c] * inv);
+        if (j + 1 <= wmax) {
+#pragma unroll
+          for (int c = j + 1; c < NPAD; ++c) {
+            if (c > wmax) break;
+            if (c <= i) R[c] = R[c] - tt * cbj[c];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (s_flag) {
+      // Cholesky failed: FP32 -> retry in FP64; FP64 -> generic LDL^T path
+      if (i == 0) {
+        if (REFINE) {
+          int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
+          P.fp64_list[p] = t;
+        } else {
+          int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
+          P.fb_list[p] = t;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    if constexpr (!REFINE) {
+      // ---- FP64: inner products of the forward-substituted columns
+      if (i < npp) {
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < C) cols[c][i] = (double)y[c];
+      }
+      __syncthreads();
+      for (int pr = i; pr < C * C; pr += NT) {
+        int a = pr / C, bb = pr % C;
+        if (bb < a) continue;
+        double s = 0.0;
+        for (int r = 0; r < npp; ++r) s = fma(cols[a][r], cols[bb][r], s);
+        G[a * C + bb] = s;
+        G[bb * C + a] = s;
+      }
+      __syncthreads();
+      if (i == 0) {
+        int fail = 0;
+        finish_outputs(P, t, G, C, zmean, &fail);
+        if (fail) {
+          int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
+          P.fb_list[p] = t;
+        } else {
+          atomicAdd(&P.counters[KK_CNT_CHOL], 1);
+        }
+      }
+      __syncthreads();
+      continue;
+    } else {
+    // ---- FP32 + FP64 refinement (REFINE)
+    // keep L (FP32) in shared memory for backward sweeps
+    if (i < npp) {
+#pragma unroll
+      for (int c = 0; c < NPAD; ++c)
+        if (c <= i) Ls[i * (i + 1) / 2 + c] = (float)R[c];
+    }
+    const int nc = P.pa + P.nvar;
+    double W[MAXC];
+    // backward sweep: x = L^-T y (right-looking over columns of L^T)
+    {
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) W[c] = 0.0;
+      float yy[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) yy[c] = (float)y[c];
+      __syncthreads();
+      for (int j = npp - 1; j >= 0; --j) {
+        float* cbj = (float*)cb[j & 1];
+        if (i == j) {
+          const float ljj = Ls[j * (j + 1) / 2 + j];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) { yy[c] = yy[c] / ljj; cbj[c] = yy[c]; }
+        }
+        __syncthreads();
+        if (i < j) {
+          const float lji = Ls[j * (j + 1) / 2 + i];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) yy[c] = yy[c] - lji * cbj[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) W[c] = c < nc ? (double)yy[c] : 0.0;
+    }
+    // refinement: r = b - K64 W (FP64), delta = K32^-1 r (FP32 sweeps)
+    int it = 0;
+    bool conv = false;
+    for (; it < 3; ++it) {
+      __syncthreads();
+      if (i < npp) {
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < nc) cols[c][i] = W[c];
+      }
+      __syncthreads();
+      double res[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) res[c] = (i < npp && c < nc) ? b[c] : 0.0;
+      if (i < npp) {
+        for (int m = 0; m < npp; ++m) {
+          const double kim = m <= i ? Kp[i * (i + 1) / 2 + m] : Kp[m * (m + 1) / 2 + i];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) res[c] = fma(-kim, cols[c][m], res[c]);
+        }
+      }
+      // forward sweep (L in shared memory), then backward sweep
+      float rr[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) rr[c] = (float)res[c];
+      for (int j = 0; j < npp; ++j) {
+        float* cbj = (float*)cb[j & 1];
+        if (i == j) {
+          const float ljj = Ls[j * (j + 1) / 2 + j];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) { rr[c] = rr[c] / ljj; cbj[c] = rr[c]; }
+        }
+        __syncthreads();
+        if (i > j && i < npp) {
+          const float lij = Ls[i * (i + 1) / 2 + j];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) rr[c] = rr[c] - lij * cbj[c];
+        }
+      }
+      for (int j = npp - 1; j >= 0; --j) {
+        float* cbj = (float*)cb[j & 1];
+        if (i == j) {
+          const float ljj = Ls[j * (j + 1) / 2 + j];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) { rr[c] = rr[c] / ljj; cbj[c] = rr[c]; }
+        }
+        __syncthreads();
+        if (i < j) {
+          const float lji = Ls[j * (j + 1) / 2 + i];
+#pragma unroll
+          for (int c = 0; c < MAXC; ++c)
+            if (c < nc) rr[c] = rr[c] - lji * cbj[c];
+        }
+      }
+      double dmax = 0.0, wmaxv = 0.0;
+      if (i < npp) {
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (c < nc) {
+            W[c] += (double)rr[c];
+            dmax = fmax(dmax, fabs((double)rr[c]));
+            wmaxv = fmax(wmaxv, fabs(W[c]));
+          }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        wmaxv = fmax(wmaxv, __shfl_xor_sync(0xffffffffu, wmaxv, o));
+      }
+      __syncthreads();
+      if ((i & 31) == 0) { red[0][i >> 5] = dmax; red[1][i >> 5] = wmaxv; }
+      __syncthreads();
+      double dm = 0.0, wm = 0.0;
+      for (int q2 = 0; q2 < NT / 32 + (NT < 32 ? 1 : 0); ++q2) { dm = fmax(dm, red[0][q2]); wm = fmax(wm, red[1][q2]); }
+      if (dm <= P.refine_tol * wm) { conv = true; ++it; break; }
+    }
+    if (i == 0) atomicAdd(&P.counters[KK_CNT_ITER], it);
+    if (!conv) {
+      if (i == 0) {
+        int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
+        P.fp64_list[p] = t;
+      }
+      __syncthreads();
+      continue;
+    }
+    // ---- FP64 outputs from the refined W = K^-1 [F k]
+    __syncthreads();
+    if (i < npp) {
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c)
+        if (c < nc) { cols[c][i] = W[c]; wvec[c][i] = b[c]; }
+      for (int u = 0; u < nu; ++u) wvec[nc + u][i] = u_entry(ts, u, i);
+    }
+    __syncthreads();
+    // G in the FP64 layout: G[a][b] = col_a^T K^-1 col_b = col_a^T W_b for
+    // a in F|k|u, b in F|k
+    for (int pr = i; pr < C * C; pr += NT) {
+      int a = pr / C, bb = pr % C;
+      if (bb >= nc && a >= nc) { G[a * C + bb] = 0.0; continue; }
+      int wa = bb < nc ? bb : a;       // the W column index
+      int va = bb < nc ? a : bb;       // the raw vector index (0..C-1)
+      const double* vec = wvec[va];
+      double s = 0.0;
+      for (int r = 0; r < npp; ++r) s = fma(vec[r], cols[wa][r], s);
+      G[a * C + bb] = s;
+    }
+    __syncthreads();
+    if (i == 0) {
+      int fail = 0;
+      finish_outputs(P, t, G, C, zmean, &fail);
+      if (fail) {
+        int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
+        P.fb_list[p] = t;
+      } else {
+        atomicAdd(&P.counters[KK_CNT_CHOL], 1);
+      }
+    }
+    __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// generic path: one thread per target, reference algorithm in global memory
+// ---------------------------------------------------------------------------
+__device__ int potrf_u(int n, double* a, int lda) {
+  for (int j = 0; j < n; ++j) {
+    double ajj = a[j + j * lda];
+    for (int k = 0; k < j; ++k) ajj = ajj - a[k + j * lda] * a[k + j * lda];
+    if (!(ajj > 0.0)) { a[j + j * lda] = ajj; return j + 1; }
+    ajj = sqrt(ajj);
+    a[j + j * lda] = ajj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = a[j + i * lda];
+      for (int k = 0; k < j; ++k) s = s - a[k + j * lda] * a[k + i * lda];
+      a[j + i * lda] = s / ajj;
+    }
+  }
+  return 0;
+}
+
+__device__ void potrs_u(int n, int nrhs, const double* a, int lda, double* b, int ldb) {
+  for (int c = 0; c < nrhs; ++c) {
+    double* x = b + (size_t)c * ldb;
+    for (int i = 0; i < n; ++i) {
+      double s = x[i];
+      for (int k = 0; k < i; ++k) s = s - a[k + i * lda] * x[k];
+      x[i] = s / a[i + i * lda];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double s = x[i];
+      for (int k = i + 1; k < n; ++k) s = s - a[i + k * lda] * x[k];
+      x[i] = s / a[i + i * lda];
+    }
+  }
+}
+
+// Bunch-Kaufman LDL^T ('U'), netlib LAPACK xSYTF2 algorithm (bundled in the
+// reference as lapack.f SSYTRF/SSYTF2), column-major m x m.
+__device__ int sytf2_u(int n, double* a, int lda, int* ipiv) {
+#define A_(i, j) a[((i) - 1) + ((j) - 1) * (size_t)lda]
+  const double alpha = (1.0 + sqrt(17.0)) / 8.0;
+  int info = 0, k = n;
+  while (k >= 1) {
+    int kstep = 1, kp;
+    double absakk = fabs(A_(k, k));
+    int imax = 0;
+    double colmax = 0.0;
+    if (k > 1) {
+      imax = 1;
+      colmax = fabs(A_(1, k));
+      for (int i = 2; i <= k - 1; ++i)
+        if (fabs(A_(i, k)) > colmax) { colmax = fabs(A_(i, k)); imax = i; }
+    }
+    if (fmax(absakk, colmax) == 0.0 || isnan(absakk)) {
+      if (info == 0) info = k;
+      kp = k;
+    } else {
+      if (absakk >= alpha * colmax) {
+        kp = k;
+      } else {
+        double rowmax = 0.0;
+        for (int j = imax + 1; j <= k; ++j) rowmax = fmax(rowmax, fabs(A_(imax, j)));
+        for (int j = 1; j <= imax - 1; ++j) rowmax = fmax(rowmax, fabs(A_(j, imax)));
+        if (absakk >= alpha * colmax * (colmax / rowmax)) kp = k;
+        else if (fabs(A_(imax, imax)) >= alpha * rowmax) kp = imax;
+        else { kp = imax; kstep = 2; }
+      }
+      int kk = k - kstep + 1;
+      if (kp != kk) {
+        for (int i = 1; i <= kp - 1; ++i) { double t = A_(i, kk); A_(i, kk) = A_(i, kp); A_(i, kp) = t; }
+        for (int j = kp + 1; j <= kk - 1; ++j) { double t = A_(j, kk); A_(j, kk) = A_(kp, j); A_(kp, j) = t; }
+        double t = A_(kk, kk); A_(kk, kk) = A_(kp, kp); A_(kp, kp) = t;
+        if (kstep == 2) { t = A_(k - 1, k); A_(k - 1, k) = A_(kp, k); A_(kp, k) = t; }
+      }
+      if (kstep == 1) {
+        double r1 = 1.0 / A_(k, k);
+        for (int j = 1; j <= k - 1; ++j) {
+          double xj = A_(j, k);
+          if (xj != 0.0) {
+            double tmp = -r1 * xj;
+            for (int i = 1; i <= j; ++i) A_(i, j) = A_(i, j) + A_(i, k) * tmp;
+          }
+        }
+        for (int i = 1; i <= k - 1; ++i) A_(i, k) = r1 * A_(i, k);
+      } else if (k > 2) {
+        double d12 = A_(k - 1, k);
+        double d22 = A_(k - 1, k - 1) / d12;
+        double d11 = A_(k, k) / d12;
+        double t = 1.0 / (d11 * d22 - 1.0);
+        d12 = t / d12;
+        for (int j = k - 2; j >= 1; --j) {
+          double wkm1 = d12 * (d11 * A_(j, k - 1) - A_(j, k));
+          double wk = d12 * (d22 * A_(j, k) - A_(j, k - 1));
+          for (int i = j; i >= 1; --i) A_(i, j) = A_(i, j) - A_(i, k) * wk - A_(i, k - 1) * wkm1;
+          A_(j, k) = wk;
+          A_(j, k - 1) = wkm1;
+        }
+      }
+    }
+    if (kstep == 1) ipiv[k - 1] = kp;
+    else { ipiv[k - 1] = -kp; ipiv[k - 2] = -kp; }
+    k -= kstep;
+  }
+  return info;
+#undef A_
+}
+
+__device__ void sytrs_u(int n, int nrhs, const double* a, int lda, const int* ipiv, double* b, int ldb) {
+#define A_(i, j) a[((i) - 1) + ((j) - 1) * (size_t)lda]
+#define B_(i, j) b[((i) - 1) + ((j) - 1) * (size_t)ldb]
+  int k = n;
+  while (k >= 1) {
+    if (ipiv[k - 1] > 0) {
+      int kp = ipiv[k - 1];
+      if (kp != k)
+        for (int j = 1; j <= nrhs; ++j) { double t = B_(k, j); B_(k, j) = B_(kp, j); B_(kp, j) = t; }
+      for (int j = 1; j <= nrhs; ++j) {
+        double bk = B_(k, j);
+        for (int i = 1; i <= k - 1; ++i) B_(i, j) = B_(i, j) - A_(i, k) * bk;
+      }
+      double r = 1.0 / A_(k, k);
+      for (int j = 1; j <= nrhs; ++j) B_(k, j) = r * B_(k, j);
+      k -= 1;
+    } else {
+      int kp = -ipiv[k - 1];
+      if (kp != k - 1)
+        for (int j = 1; j <= nrhs; ++j) { double t = B_(k - 1, j); B_(k - 1, j) = B_(kp, j); B_(kp, j) = t; }
+      for (int j = 1; j <= nrhs; ++j) {
+        double bk = B_(k, j), bkm1 = B_(k - 1, j);
+        for (int i = 1; i <= k - 2; ++i) B_(i, j) = B_(i, j) - A_(i, k) * bk;
+        for (int i = 1; i <= k - 2; ++i) B_(i, j) = B_(i, j) - A_(i, k - 1) * bkm1;
+      }
+      double akm1k = A_(k - 1, k);
+      double akm1 = A_(k - 1, k - 1) / akm1k;
+      double ak = A_(k, k) / akm1k;
+      double denom = akm1 * ak - 1.0;
+      for (int j = 1; j <= nrhs; ++j) {
+        double bkm1 = B_(k - 1, j) / akm1k;
+        double bk = B_(k, j) / akm1k;
+        B_(k - 1, j) = (ak * bkm1 - bk) / denom;
+        B_(k, j) = (akm1 * bk - bkm1) / denom;
+      }
+      k -= 2;
+    }
+  }
+  k = 1;
+  while (k <= n) {
+    if (ipiv[k - 1] > 0) {
+      for (int j = 1; j <= nrhs; ++j) {
+        double s = 0.0;
+        for (int i = 1; i <= k - 1; ++i) s = s + A_(i, k) * B_(i, j);
+        B_(k, j) = B_(k, j) - s;
+      }
+      int kp = ipiv[k - 1];
+      if (kp != k)
+        for (int j = 1; j <= nrhs; ++j) { double t = B_(k, j); B_(k, j) = B_(kp, j); B_(kp, j) = t; }
+      k += 1;
+    } else {
+      for (int j = 1; j <= nrhs; ++j) {
+        double s = 0.0, s1 = 0.0;
+        for (int i = 1; i <= k - 1; ++i) s = s + A_(i, k) * B_(i, j);
+        for (int i = 1; i <= k - 1; ++i) s1 = s1 + A_(i, k + 1) * B_(i, j);
+        B_(k, j) = B_(k, j) - s;
+        B_(k + 1, j) = B_(k + 1, j) - s1;
+      }
+      int kp = -ipiv[k - 1];
+      if (kp != k)
+        for (int j = 1; j <= nrhs; ++j) { double t = B_(k, j); B_(k, j) = B_(kp, j); B_(kp, j) = t; }
+      k += 2;
+    }
+  }
+#undef A_
+#undef B_
+}
+
+// one target, reference algorithm (solve_linear_system_base,
+// kriging_base.F90:3244-3398) including the SSYTRF + jitter ladder
+__global__ void k_solve_generic(SolveParams P, const int* __restrict__ list, const int* __restrict__ list_count) {
+  const int n_items = *list_count;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  double* ws = P.scratch + (size_t)gt * P.scratch_stride;
+  for (int item = gt; item < n_items; item += gridDim.x * blockDim.x) {
+    const int t = list[item];
+    const int q = P.nvar, pa = P.pa;
+    int nn[KK_MAXVAR], ist[KK_MAXVAR], npp = 0;
+    for (int v = 0; v < q; ++v) { nn[v] = P.nnear[v][t]; ist[v] = npp; npp += nn[v]; }
+    const int m = npp + pa;
+    const double rs = P.rs ? P.rs[t] : 1.0, ln = P.ln ? P.ln[t] : 0.0;
+    double* A = ws;
+    double* Bm = A + (size_t)m * m;          // (q, m)
+    double* X = Bm + (size_t)q * m;          // (q, m)
+    double* L = X + (size_t)q * m;           // (npp, npp)
+    double* Y = L + (size_t)m * m;           // (npp, pa); L doubles as the m x m LDL^T factor
+    double* S = Y + (size_t)npp * (pa > 0 ? pa : 1);
+    double* Z = S + (size_t)(pa > 0 ? pa * pa : 1);  // (m, q)
+    double* rsm = Z + (size_t)m * q;         // (pa, q)
+    int* ipiv = (int*)(rsm + (size_t)(pa > 0 ? pa : 1) * q + 1);
+    auto row_vo = [&](int r, int& v, int& o) {
+      v = 0;
+      while (v + 1 < q && r >= ist[v + 1]) ++v;
+      o = P.nbr[v][(size_t)t * P.mmax[v] + (r - ist[v])];
+    };
+    auto xcoord = [&](int v, int o, double* x) { for (int d = 0; d < P.nlag; ++d) x[d] = P.ox[v][d][o]; };
+    // RHS
+    for (int iv = 0; iv < q; ++iv) {
+      for (int r = 0; r < npp; ++r) {
+        int v, o;
+        row_vo(r, v, o);
+        double xr[4];
+        xcoord(v, o, xr);
+        double tmp = 0.0;
+        int k0 = P.gstart ? P.gstart[t] : 0, k1 = P.gstart ? P.gstart[t + 1] : 1;
+        for (int k = k0; k < k1; ++k) {
+          double node[4], lag[4];
+          for (int d = 0; d < P.nlag; ++d) node[d] = P.gstart ? P.gx[d][k] : P.tx[d][t];
+          make_lag(P, xr, node, rs, lag);
+          tmp = dadd(tmp, dmul(cov_pair(P, v, iv, lag), P.gstart ? P.gw[k] : 1.0));
+        }
+        Bm[iv + (size_t)r * q] = tmp;
+      }
+      for (int a = 0; a < pa; ++a) Bm[iv + (size_t)(npp + a) * q] = g_entry(P, a, iv, t);
+    }
+    // LHS lower + mirror
+    for (size_t e = 0; e < (size_t)m * m; ++e) A[e] = 0.0;
+    for (int c = 0; c < npp; ++c) {
+      int vc, oc;
+      row_vo(c, vc, oc);
+      double xc[4];
+      xcoord(vc, oc, xc);
+      A[c + (size_t)c * m] = dadd(dadd(cov0_pair(P, vc, vc), P.ovar[vc][oc]), ln);
+      for (int r = c + 1; r < npp; ++r) {
+        int vr, orr;
+        row_vo(r, vr, orr);
+        double xr[4], lag[4];
+        xcoord(vr, orr, xr);
+        make_lag(P, xc, xr, rs, lag);
+        A[r + (size_t)c * m] = cov_pair(P, vr, vc, lag);
+      }
+      for (int a = 0; a < pa; ++a) A[(npp + a) + (size_t)c * m] = f_entry(P, a, vc, oc);
+    }
+    for (int ir = 0; ir < npp; ++ir)
+      for (int ic = ir + 1; ic < m; ++ic) A[ir + (size_t)ic * m] = A[ic + (size_t)ir * m];
+    // kriging_setup + kriging_solve_prepared (solver.f90:224-300)
+    for (int j = 0; j < npp; ++j)
+      for (int r = 0; r < npp; ++r) L[r + (size_t)j * npp] = A[r + (size_t)j * m];
+    int info = potrf_u(npp, L, npp);
+    if (info == 0 && pa > 0) {
+      for (int j = 0; j < pa; ++j)
+        for (int r = 0; r < npp; ++r) Y[r + (size_t)j * npp] = A[r + (size_t)(npp + j) * m];
+      potrs_u(npp, pa, L, npp, Y, npp);
+      for (int j = 0; j < pa; ++j)
+        for (int r = 0; r < pa; ++r) {
+          double s = 0.0;
+          for (int k = 0; k < npp; ++k) s = s + A[k + (size_t)(npp + r) * m] * Y[k + (size_t)j * npp];
+          S[r + (size_t)j * pa] = s;
+        }
+      info = potrf_u(pa, S, pa);
+    }
+    if (info == 0) {
+      for (int c = 0; c < q; ++c)
+        for (int k = 0; k < npp; ++k) Z[k + (size_t)c * npp] = Bm[c + (size_t)k * q];
+      potrs_u(npp, q, L, npp, Z, npp);
+      if (pa == 0) {
+        for (int c = 0; c < q; ++c)
+          for (int k = 0; k < npp; ++k) X[c + (size_t)k * q] = Z[k + (size_t)c * npp];
+      } else {
+        for (int c = 0; c < q; ++c)
+          for (int a = 0; a < pa; ++a) {
+            double s = 0.0;
+            for (int k = 0; k < npp; ++k) s = s + Y[k + (size_t)a * npp] * Bm[c + (size_t)k * q];
+            rsm[a + (size_t)c * pa] = s - Bm[c + (size_t)(npp + a) * q];
+          }
+        potrs_u(pa, q, S, pa, rsm, pa);
+        for (int c = 0; c < q; ++c) {
+          for (int k = 0; k < npp; ++k) {
+            double s = 0.0;
+            for (int a = 0; a < pa; ++a) s = s + Y[k + (size_t)a * npp] * rsm[a + (size_t)c * pa];
+            X[c + (size_t)k * q] = Z[k + (size_t)c * npp] - s;
+          }
+          for (int a = 0; a < pa; ++a) X[c + (size_t)(npp + a) * q] = rsm[a + (size_t)c * pa];
+        }
+      }
+      atomicAdd(&P.counters[KK_CNT_CHOL], 1);
+    } else {
+      // SSYTRF on the augmented system, jitter retry (kriging_base.F90:3289-3342)
+      double* Af = L;  // reuse (needs m*m: workspace sized for it)
+      for (size_t e = 0; e < (size_t)m * m; ++e) Af[e] = A[e];
+      info = sytf2_u(m, Af, m, ipiv);
+      if (info != 0 && npp > 0) {
+        double dscale = 0.0;
+        for (int ii = 0; ii < npp; ++ii) dscale = dscale + A[ii + (size_t)ii * m];
+        if (dscale > 0.0) {
+          dscale = 1.0e-6 * (dscale / (double)npp);
+          for (int ii = 0; ii < npp; ++ii) A[ii + (size_t)ii * m] = A[ii + (size_t)ii * m] + dscale;
+          for (size_t e = 0; e < (size_t)m * m; ++e) Af[e] = A[e];
+          info = sytf2_u(m, Af, m, ipiv);
+        }
+      }
+      if (info == 0) {
+        for (int c = 0; c < q; ++c)
+          for (int k = 0; k < m; ++k) Z[k + (size_t)c * m] = Bm[c + (size_t)k * q];
+        sytrs_u(m, q, Af, m, ipiv, Z, m);
+        for (int c = 0; c < q; ++c)
+          for (int k = 0; k < m; ++k) X[c + (size_t)k * q] = Z[k + (size_t)c * m];
+        atomicAdd(&P.counters[KK_CNT_LDLT], 1);
+      }
+    }
+    if (info != 0) {
+      atomicAdd(&P.counters[KK_CNT_FAIL], 1);
+      P.status[t] |= KK_ST_FAIL;
+      write_nan(P, t);
+      continue;
+    }
+    // calc_variance + estimate_block_base
+    double* Vt = P.var + (size_t)t * q * q;
+    for (int iv = 0; iv < q; ++iv)
+      for (int jv = iv; jv < q; ++jv) {
+        double s = 0.0;
+        for (int k = 0; k < m; ++k) s = s + X[iv + (size_t)k * q] * Bm[jv + (size_t)k * q];
+        double v = base_cov(P, t, iv, jv) - s;
+        Vt[iv + jv * q] = v;
+        Vt[jv + iv * q] = v;
+      }
+    for (int iv = 0; iv < q; ++iv) {
+      if (Vt[iv + iv * q] < 0.0) Vt[iv + iv * q] = 0.0;
+      for (int jv = iv + 1; jv < q; ++jv) {
+        double o = Vt[jv + iv * q];
+        if (o < 0.0) o = 0.0;
+        Vt[jv + iv * q] = o;
+        Vt[iv + jv * q] = o;
+      }
+    }
+    double tmean[KK_MAXVAR];
+    for (int v = 0; v < q; ++v) {
+      double s = 0.0;
+      for (int k = 0; k < nn[v]; ++k) s = s + P.oval[v][P.nbr[v][(size_t)t * P.mmax[v] + k]];
+      tmean[v] = nn[v] > 0 ? s / nn[v] : 0.0;
+    }
+    for (int jv = 0; jv < q; ++jv) {
+      double tw[KK_MAXVAR], avg = 0.0, tws = 0.0;
+      for (int v = 0; v < q; ++v) {
+        double sw = 0.0, dp = 0.0;
+        for (int k = 0; k < nn[v]; ++k) {
+          double wt = X[jv + (size_t)(ist[v] + k) * q];
+          sw = sw + wt;
+          dp = dp + P.oval[v][P.nbr[v][(size_t)t * P.mmax[v] + k]] * wt;
+        }
+        tw[v] = sw;
+        tws += sw;
+        avg = avg + dp;
+        if (P.ck_isa && v != jv && nn[v] > 0) avg = avg + (tmean[jv] - tmean[v]) * tw[v];
+      }
+      if (P.unbias == 0 && P.sk_mean[jv] != 0.0) avg = avg + (1.0 - tws) * P.sk_mean[jv];
+      if (avg < P.bounds[0]) avg = P.bounds[0];
+      if (avg > P.bounds[1]) avg = P.bounds[1];
+      P.est[(size_t)t * q + jv] = avg;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T, int NPAD, bool REFINE>
+static void launch_reg(const SolveParams& P, const int* list, const int* cnt, int slot, int nsm, cudaStream_t st) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_reg<T, NPAD, REFINE>, NPAD, 0);
+  if (occ < 1) occ = 1;
+  k_solve_reg<T, NPAD, REFINE><<<nsm * occ, NPAD, 0, st>>>(P, list, cnt, slot);
+}
+
+void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm, cudaStream_t st) {
+  const int* c = P.counters;
+  const int* l32 = lists + (size_t)KK_CNT_B16 * P.nblock;
+  const int* l64 = lists + (size_t)KK_CNT_B64 * P.nblock;
+  if (precision == 0) {
+    launch_reg<double, 32, false>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
+    launch_reg<double, 64, false>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
+  } else {
+    launch_reg<float, 32, true>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
+    launch_reg<float, 64, true>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
+  }
+}
+
+// FP64 register solve of an explicit list (FP32 non-convergence fallback):
+// the list is split by size inside the kernel via the padding bound
+void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_slot, int nsm, cudaStream_t st) {
+  launch_reg<double, 64, false>(P, list, P.counters + list_cnt_slot, KK_CNT_WORK0 + 2, nsm, st);
+}
+
+void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st) {
+  int blocks = (nthreads + 63) / 64;
+  k_solve_generic<<<blocks, 64, 0, st>>>(P, list, P.counters + list_cnt_slot);
+}
+
+}  // namespace kk
