@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark: kriged targets/s on one B200 for the 2-D anisotropic sector-search
+ordinary-kriging workload (200 000 clustered observations, 2000 x 2000 targets).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  ``value`` is device throughput of the FP32-factor +
+FP64-refinement form with inputs resident in HBM (CUDA events on the solve
+stream, L2 flushed between timed steps, max over ranks); ``fp64_plain`` is the
+same measurement for the FP64 form; ``e2e`` is the same metric through the
+public ``Kriging`` API with host inputs/outputs copied every step.  The
+reference arm (``--impl reference``) times the CPU restatement of the
+reference engine (oracle/kk_oracle.c, OpenMP over all host threads) on a
+bounded contiguous sample of the same targets.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import bench_workloads as bw  # noqa: E402
+
+METRIC = "kriged targets/s on 1 B200: FP32+refine batched vs FP64 plain at <=1e-6 rel err"
+
+
+def solve_flops(n, p=1, q=1):
+    """Algorithmic FLOPs of one target system (Cholesky n^3/3, solves, Schur, variance)."""
+    n = np.asarray(n, dtype=np.float64)
+    return (n ** 3 / 3 + n ** 2 / 2 + n / 6 + 2 * n ** 2 * (p + q) + 2 * n * p ** 2 + 4 * n * p * q
+            + p ** 3 / 3 + 2 * p ** 2 * q + 2 * (n + p) * q ** 2 + 2 * n * q)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks(torch, device):
+    """Live cuBLAS SGEMM (FP32 CUDA cores, TF32 off) and DGEMM throughput, TFLOP/s."""
+    out = {}
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for name, dt, n in (("fp32", torch.float32, 8192), ("fp64", torch.float64, 8192)):
+        a = torch.randn(n, n, device=device, dtype=dt)
+        b = torch.randn(n, n, device=device, dtype=dt)
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out[name] = 2.0 * n ** 3 / best / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = old
+    torch.cuda.empty_cache()
+    return out
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def cpu_sample_run(w, nthread, target_seconds, precision_ref=None):
+    """Time the CPU oracle on a contiguous slab of targets (all observations)."""
+    from oracle.oracle import OracleKriging
+    grid = w["grid"]
+
+    def run(lo, hi):
+        o = OracleKriging(ndim=w["ndim"], nvar=w["nvar"], nmin=w.get("nmin", 0), **w["kw"])
+        bw.apply(o, w, set_grid=False)
+        o.set_grid(grid[lo:hi])
+        t0 = time.perf_counter()
+        o.solve(nthread=nthread)
+        return time.perf_counter() - t0, o
+
+    pilot = min(len(grid), 4000)
+    lo0 = (len(grid) // 2) - (len(grid) // 2) % 2000
+    dt, _ = run(lo0, lo0 + pilot)
+    rate = pilot / max(dt, 1e-6)
+    n = int(min(len(grid) - lo0, max(pilot, rate * target_seconds)))
+    dt, o = run(lo0, lo0 + n)
+    return dict(rate=n / dt, seconds=dt, lo=lo0, hi=lo0 + n, oracle=o)
+
+
+def run_reference(args, w):
+    nthread = os.cpu_count() or 1
+    step_rates = []
+    for _ in range(args.warmup):
+        cpu_sample_run(w, nthread, args.cpu_seconds / 4)
+    last = None
+    for _ in range(args.steps):
+        r = cpu_sample_run(w, nthread, args.cpu_seconds)
+        step_rates.append(r["rate"])
+        last = r
+    value = statistics.median(step_rates)
+    sample = (f"targets {last['lo']}..{last['hi']} (rows of the 2000x2000 grid) with all "
+              f"{len(w['obs'][0]['coord'])} observations; {last['seconds']:.1f} s per step")
+    line = {
+        "metric": METRIC, "value": value, "unit": "targets/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": last["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, see bench_workloads.py)",
+        "config": {"workload": w["name"], "ntargets": int(len(w["grid"])),
+                   "nobs": int(len(w["obs"][0]["coord"])), "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "targets/s", "cores": nthread, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=2000, help="targets per axis (default: the benchmark's 2000)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w = bw.config2(grid_n=args.grid)
+        run_reference(args, w)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from krigekit_b200 import Kriging
+
+    w = bw.config2(grid_n=args.grid)
+    ntarget = len(w["grid"])
+    nobs = len(w["obs"][0]["coord"])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def time_steps(k, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            k.solve()
+        barrier()
+        times = []
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            for _ in range(steps):
+                flush.fill_(1.0)  # L2 flush between timed steps (256 MiB write, outside the timed region)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                k.solve()
+                e1.record()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        barrier()
+        tot = sum(times) / 1e3
+        if dist is not None:
+            t = torch.tensor([tot], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        return tot, times
+
+    def make(precision):
+        k = Kriging(ndim=2, nvar=1, precision=precision, nmin=w["nmin"], **w["kw"])
+        bw.apply(k, w)
+        return k
+
+    # ---- FP32 + refinement (the measured form)
+    k32 = make("fp32_refine")
+    sampler = ClockSampler(dev)
+    tot32, times32 = time_steps(k32, args.steps, args.warmup, sampler)
+    value = ntarget * world * args.steps / tot32
+    clocks = sampler.summary()
+    # per-phase device times from one extra profiled solve
+    k32.profile(True)
+    flush.fill_(1.0)
+    k32.solve()
+    ph32 = k32.phases()
+    k32.profile(False)
+    gst = k32.gpu_stats()
+    e32, v32 = k32.get_results()
+    nnear, _ = k32.get_neighbours(1)
+
+    # ---- FP64 plain
+    fp64 = None
+    if not args.no_fp64:
+        k64 = make("fp64")
+        tot64, _ = time_steps(k64, args.steps, args.warmup)
+        k64.profile(True)
+        flush.fill_(1.0)
+        k64.solve()
+        ph64 = k64.phases()
+        e64, v64 = k64.get_results()
+        fp64 = {"value": ntarget * world * args.steps / tot64, "ms_per_step": tot64 / args.steps * 1e3,
+                "phases_ms": ph64}
+        ee = bw.rel_err(e32, e64, 1e-3 * w["zstd"])
+        ve = bw.rel_err(v32, v64, 1e-3 * w["sill"])
+        fin = np.isfinite(e64)
+        fp64["fp32_vs_fp64_rel_err"] = {
+            "est_max": float(ee[fin].max()), "est_p99": float(np.percentile(ee[fin], 99)),
+            "var_max": float(ve[fin].max()), "var_p99": float(np.percentile(ve[fin], 99))}
+        del k64
+
+    # ---- roofline of the dominant kernel (the FP32 solve kernels)
+    peaks = measured_peaks(torch, dev)
+    nn = nnear[nnear >= 2].astype(np.float64)
+    flops = float(solve_flops(nn).sum())
+    achieved = flops / (ph32["solve_ms"] / 1e3) / 1e12
+    hbm_gbs, hbm_src = hbm_peak()
+    # search: algorithmic bytes = target coords + neighbour gathers (8*(ndim+1) per neighbour) + list write
+    search_bytes = ntarget * 16 + float(nn.sum()) * (8 * 3 + 4) + ntarget * 4
+    search_gbs = search_bytes / (ph32["search_ms"] / 1e3) / 1e9
+
+    # ---- CPU baseline (oracle on a bounded sample) + accuracy against it
+    cpu = None
+    acc = None
+    if rank == 0 and not args.no_cpu:
+        r = cpu_sample_run(w, os.cpu_count() or 1, args.cpu_seconds)
+        o = r["oracle"]
+        lo, hi = r["lo"], r["hi"]
+        oe, ov = o.get_results()
+        ee = bw.rel_err(e32[lo:hi], oe, 1e-3 * w["zstd"])
+        ve = bw.rel_err(v32[lo:hi], ov, 1e-3 * w["sill"])
+        _, inear32 = k32.get_neighbours(1)
+        same = bool(np.array_equal(nnear[lo:hi], o.nnear[:, 0]))
+        if same:
+            m = inear32.shape[1]
+            same = bool(np.array_equal(inear32[lo:hi, :m], o.inear[:, 0, :m]))
+        acc = {"vs_oracle_sample": f"targets {lo}..{hi}", "est_max": float(ee.max()),
+               "est_p99": float(np.percentile(ee, 99)), "var_max": float(ve.max()),
+               "var_p99": float(np.percentile(ve, 99)), "neighbour_sets_identical": same}
+        cpu = {"value": r["rate"], "unit": "targets/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"targets {lo}..{hi} of the 2000x2000 grid, all {nobs} observations, "
+                         f"{r['seconds']:.1f} s (oracle/kk_oracle.c, OpenMP dynamic,1, 64-slot factor cache)"}
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        obs = w["obs"][0]
+        k = Kriging(ndim=2, nvar=1, precision="fp32_refine", nmin=w["nmin"], **w["kw"])
+        for (i, j, spec) in w["vgm"]:
+            k.set_vgm(i, j, **spec)
+
+        def e2e_step():
+            k.set_obs(1, obs["coord"], obs["value"], nmax=obs["nmax"])
+            k.set_grid(w["grid"])
+            k.set_search(1, **w["search"][0])
+            k.solve()
+            return k.get_results()
+
+        for _ in range(max(1, args.warmup - 1)):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        h2d = nobs * (2 * 8 + 8 + 8) + ntarget * 2 * 8
+        d2h = ntarget * 8 * 2
+        e2e = {"value": ntarget * world * args.steps / te, "unit": "targets/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": te / args.steps * 1e3,
+               "note": "pageable numpy inputs through Kriging.set_obs/set_grid/solve/get_results"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot32 / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refinement",
+            "data": "synthetic (seeded, see bench_workloads.py)",
+            "config": {"workload": w["name"], "ntargets": ntarget, "nobs": nobs,
+                       "search": "anisotropic (0.5, az 30), 4 sectors x 16", "variogram": "exp r0.1 nug0.02",
+                       "precision": "fp32_refine", "l2": "flushed (256 MiB write) between timed steps",
+                       "parallelism": f"targets replicated per rank (weak), {world} GPU(s)"},
+            "fp64_plain": fp64,
+            "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,
+            "accuracy": acc,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
+                         "frac": achieved / peaks["fp32"], "traffic": None,
+                         "kernel": "k_solve_reg<float,32|64,refine> (solve phase)",
+                         "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live",
+                         "flops_per_solve": flops, "solve_ms": ph32["solve_ms"]},
+            "roofline_search": {"bound": "hbm", "achieved": search_gbs, "peak": hbm_gbs, "unit": "GB/s",
+                                "frac": search_gbs / hbm_gbs, "traffic": None, "peak_source": hbm_src,
+                                "search_ms": ph32["search_ms"]},
+            "peaks_measured_tflops": peaks,
+            "phases_ms": ph32, "gpu_stats": gst,
+            "gpu_launches": int(ph32["launches"] * args.steps),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    main()

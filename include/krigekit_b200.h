@@ -114,6 +114,12 @@ int krige_get_status(int64_t handle, int nblocks, int *status);
  * FP64 re-solves, refinement iterations; solve_ms = wall time of krige_solve. */
 int krige_gpu_stats(int64_t handle, int *out8, double *solve_ms);
 
+/* Enable per-phase CUDA-event timing of krige_solve (one event sync per phase). */
+int krige_gpu_profile(int64_t handle, int enable);
+/* Device ms per phase of the last solve: search, bucket, solve kernels, fallbacks;
+ * launches = kernels launched by that solve. */
+int krige_gpu_phases(int64_t handle, double *out4, int *launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,8 +6,10 @@ device is visible.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes
 import os
+import weakref
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libkrigecuda.so")
@@ -78,6 +80,8 @@ SIGNATURES = {
     "krige_get_mmax": ([_c_i64, _c_int, _p_int], _c_int),
     "krige_get_status": ([_c_i64, _c_int, _p_int], _c_int),
     "krige_gpu_stats": ([_c_i64, _p_int, _p_dbl], _c_int),
+    "krige_gpu_profile": ([_c_i64, _c_int], _c_int),
+    "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),
 }
 
 _lib = None
@@ -143,3 +147,22 @@ def use_torch_allocator() -> None:
     _alloc_cb = ALLOC_FN(_alloc)
     _free_cb = FREE_FN(_free)
     load().krige_set_allocator(_alloc_cb, _free_cb, None)
+
+
+# -- handles alive at interpreter exit ----------------------------------------
+_live = weakref.WeakSet()
+
+
+def register(obj) -> None:
+    """Track an object owning a handle; its ``close()`` runs at interpreter exit."""
+    _live.add(obj)
+
+
+@atexit.register
+def _close_all() -> None:
+    # Destroy engines while torch and the allocator callbacks still exist.
+    for obj in list(_live):
+        try:
+            obj.close()
+        except Exception:
+            pass

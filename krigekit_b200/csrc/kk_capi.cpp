@@ -36,7 +36,10 @@ bool failed() {
   return !g_err.empty();
 }
 
-static std::vector<std::unique_ptr<Engine>> g_reg;
+// The registry is never destroyed: engines still alive at process exit keep
+// their device buffers, because the allocator callbacks they would call (a
+// Python allocator, for instance) may already be gone by then.
+static std::vector<std::unique_ptr<Engine>>& g_reg = *new std::vector<std::unique_ptr<Engine>>();
 static std::mutex g_reg_mu;
 
 static Engine* get(int64_t h) {
@@ -603,6 +606,26 @@ int krige_gpu_stats(int64_t h, int* out8, double* solve_ms) {
   if (!e) return 1;
   for (int i = 0; i < 8; ++i) out8[i] = e->stats[i];
   if (solve_ms) *solve_ms = e->last_solve_ms;
+  KK_GUARD_END
+}
+
+// Enable per-phase CUDA-event timing of solve() (adds one event sync per phase).
+int krige_gpu_profile(int64_t h, int enable) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  e->profile = enable ? 1 : 0;
+  KK_GUARD_END
+}
+
+// Device time per phase of the last solve (ms): search, bucket, solve kernels,
+// fallbacks (kd-tree replica, FP64 re-solve, generic); kernel launches.
+int krige_gpu_phases(int64_t h, double* out4, int* launches) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  for (int i = 0; i < 4; ++i) out4[i] = e->phase_ms[i];
+  if (launches) *launches = e->launches;
   KK_GUARD_END
 }
 

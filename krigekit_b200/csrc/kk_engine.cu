@@ -142,7 +142,11 @@ static void build_grid(Engine& e, int v) {
   }
   g.G = std::min(D, 3);
   g.nobs = n;
-  // cell size for about two points per cell on average
+  // Cell size from the dense end of the point distribution: a coarse
+  // histogram gives the density seen by the 99th-percentile point, and cells
+  // are sized to hold about max(2, K/8) points there, so a K-nearest search
+  // in the densest regions gathers a few K candidates while sparse regions
+  // cost only extra (cheap, mostly empty) cell rows.
   double ext[3], vol = 1.0, emax = 0.0;
   for (int k = 0; k < g.G; ++k) emax = std::max(emax, g.umax[k] - g.umin[k]);
   if (emax <= 0.0) emax = 1.0;
@@ -150,16 +154,42 @@ static void build_grid(Engine& e, int v) {
     ext[k] = std::max(g.umax[k] - g.umin[k], 1e-9 * emax);
     vol *= ext[k];
   }
-  const double occ = 2.0;
-  double hcell = std::pow(vol * occ / std::max(n, 1), 1.0 / g.G);
+  const int nc_axis = g.G == 1 ? 65536 : (g.G == 2 ? 256 : 48);
+  long long ncoarse = 1;
+  for (int k = 0; k < g.G; ++k) ncoarse *= nc_axis;
+  std::vector<int> coarse(ncoarse, 0);
+  for (int i = 0; i < n; ++i) {
+    long long c = 0, stride = 1;
+    for (int k = 0; k < g.G; ++k) {
+      int ck = (int)((h[(size_t)k * n + i] - g.umin[k]) / ext[k] * nc_axis);
+      ck = ck < 0 ? 0 : (ck >= nc_axis ? nc_axis - 1 : ck);
+      c += ck * stride;
+      stride *= nc_axis;
+    }
+    coarse[c]++;
+  }
+  std::vector<int> cnt;
+  cnt.reserve(4096);
+  for (int v : coarse) if (v > 0) cnt.push_back(v);
+  std::sort(cnt.begin(), cnt.end());
+  long long acc = 0, p99 = 0;
+  for (size_t q = 0; q < cnt.size(); ++q) {  // density of the cell holding the 99th-percentile point
+    acc += cnt[q];
+    if (acc >= (long long)(0.99 * n)) { p99 = cnt[q]; break; }
+  }
+  const double coarse_vol = vol / (double)ncoarse;
+  const double rho = std::max((double)p99, 1.0) / coarse_vol;
+  const double occ = std::max(2.0, S.K / 8.0);
+  double hcell = std::pow(occ / rho, 1.0 / g.G);
+  hcell = std::max(hcell, std::pow(vol * 2.0 / std::max(n, 1), 1.0 / g.G) * 0.05);
   long long ncell = 1;
   for (int k = 0; k < g.G; ++k) {
     long long c = (long long)std::ceil(ext[k] / hcell);
-    c = std::max<long long>(1, std::min<long long>(c, 1 << 14));
+    c = std::max<long long>(1, std::min<long long>(c, g.G == 1 ? (1 << 24) : (1 << 14)));
     g.n[k] = (int)c;
     ncell *= c;
   }
-  while (ncell > (1ll << 26)) {
+  while (ncell > (1ll << 25)) {
     ncell = 1;
     for (int k = 0; k < g.G; ++k) { g.n[k] = std::max(1, g.n[k] / 2); ncell *= g.n[k]; }
   }
@@ -247,12 +277,36 @@ static void validate(const Engine& e) {
       }
 }
 
+// CUDA-event timer for the solve phases (enabled by krige_gpu_profile)
+struct PhaseTimer {
+  Engine& e;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  explicit PhaseTimer(Engine& en) : e(en) {
+    if (e.profile) { cudaEventCreate(&ev[0]); cudaEventCreate(&ev[1]); }
+  }
+  ~PhaseTimer() {
+    if (ev[0]) { cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]); }
+  }
+  void start() { if (ev[0]) cudaEventRecord(ev[0], e.stream); }
+  void stop(int phase) {
+    if (!ev[0]) return;
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventSynchronize(ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    e.phase_ms[phase] += ms;
+  }
+};
+
 void engine_solve(Engine& e) {
   auto t0 = std::chrono::steady_clock::now();
+  for (double& x : e.phase_ms) x = 0.0;
+  e.launches = 0;
   e.solved = false;
   std::memset(e.stats, 0, sizeof e.stats);
   validate(e);
   KK_CUDA(cudaSetDevice(e.device));
+  PhaseTimer timer(e);
   cudaStream_t st = e.stream;
   const int nsm = sm_count(e.device);
   set_zones(st);
@@ -359,9 +413,12 @@ void engine_solve(Engine& e) {
     const double* tx[4] = {e.tx[0].as<double>(), e.tx[1].as<double>(), e.tx[2].as<double>(), e.tx[3].as<double>()};
     const double* ox[4] = {d.x[0].as<double>(), d.x[1].as<double>(), d.x[2].as<double>(), d.x[3].as<double>()};
     KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + KK_CNT_REDO + v, 0, sizeof(int), st));
+    timer.start();
     launch_search(S, nb, tx, ox, d.nbr.as<int>(), d.nnear.as<int>(), e.status.as<int>(), redo,
                   e.counters.as<int>() + KK_CNT_REDO + v, nsm, st);
     KK_CUDA(cudaGetLastError());
+    timer.stop(0);
+    e.launches += 1;
     int nredo = 0;
     KK_CUDA(cudaMemcpyAsync(&nredo, e.counters.as<int>() + KK_CNT_REDO + v, sizeof(int), cudaMemcpyDeviceToHost, st));
     KK_CUDA(cudaStreamSynchronize(st));
@@ -372,9 +429,12 @@ void engine_solve(Engine& e) {
       const int stride = S.K + 2;
       DBuf heaps;
       heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);
+      timer.start();
       launch_search_kdtree(S, redo, e.counters.as<int>() + KK_CNT_REDO + v, tx, ox, d.nbr.as<int>(),
                            d.nnear.as<int>(), e.status.as<int>(), heaps.p, stride, nthreads, st);
       KK_CUDA(cudaGetLastError());
+      timer.stop(3);
+      e.launches += 1;
       KK_CUDA(cudaStreamSynchronize(st));
     }
   }
@@ -435,13 +495,21 @@ void engine_solve(Engine& e) {
     throw std::string("too many drift/variable columns for the register kernels (max 8)");
 
   // ---- bucket + solve
+  timer.start();
   launch_bucket(P, e.bucket.as<int>(), st);
+  timer.stop(1);
+  timer.start();
   launch_solve(P, e.precision, e.bucket.as<int>(), nsm, st);
   KK_CUDA(cudaGetLastError());
+  timer.stop(2);
+  e.launches += 3;
   if (e.precision != 0) {
     // FP32 targets whose refinement did not converge: FP64 register kernel
+    timer.start();
     launch_solve_fp64_list(P, P.fp64_list, KK_CNT_FP64, nsm, st);
     KK_CUDA(cudaGetLastError());
+    timer.stop(3);
+    e.launches += 1;
   }
   int cnt[KK_CNT_N];
   KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
@@ -456,10 +524,17 @@ void engine_solve(Engine& e) {
     e.scratch.reserve(sizeof(double) * stride * nthreads);
     P.scratch = e.scratch.as<double>();
     P.scratch_stride = (int)stride;
-    if (nbig > 0)
+    timer.start();
+    if (nbig > 0) {
       launch_solve_generic(P, e.bucket.as<int>() + (size_t)KK_CNT_BIG * nb, KK_CNT_BIG, std::min(nbig, 2048), st);
-    if (nfb > 0) launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(nfb, 2048), st);
+      e.launches += 1;
+    }
+    if (nfb > 0) {
+      launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(nfb, 2048), st);
+      e.launches += 1;
+    }
     KK_CUDA(cudaGetLastError());
+    timer.stop(3);
     KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
     KK_CUDA(cudaStreamSynchronize(st));
   }

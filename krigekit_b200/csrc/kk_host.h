@@ -97,6 +97,11 @@ struct Engine {
   bool solved = false;
   int stats[8] = {0};
   double last_solve_ms = 0.0;
+  // per-phase device time of the last solve (CUDA events on the handle's
+  // stream): search, bucket, solve kernels, fallbacks; and kernel launches
+  int profile = 0;
+  double phase_ms[4] = {0, 0, 0, 0};
+  int launches = 0;
 
   int naug() const { return std_ck ? unbias * nvar : unbias; }
   int pdrift() const { return ndrift + naug(); }

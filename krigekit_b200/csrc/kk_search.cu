@@ -778,7 +778,6 @@ __global__ void k_search_kdtree(KkSearch S, const int* __restrict__ list, const 
       out[j + 1] = tmp;
     }
     nnear[t] = nsel;
-    status[t] = 0;
   }
 }
 

@@ -190,7 +190,7 @@ __device__ double base_cov(const SolveParams& P, int t, int iv, int jv) {
 // Solve the small p x p Schur system and produce est / var from the inner
 // products G (FP64).  Column order: F (pa), k (nvar), u (nu).
 // G is symmetric, stored full C x C.
-__device__ void finish_outputs(const SolveParams& P, int t, const double* G, int C, const double* zmean,
+__device__ __noinline__ void finish_outputs(const SolveParams& P, int t, const double* G, int C, const double* zmean,
                                int* fail) {
   const int pa = P.pa, q = P.nvar, nu = n_func(P);
   const int kF = 0, kK = pa, kU = pa + q;
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(NPAD, 1) k_solve_reg(SolveParams P, const int*
   constexpr int NK = NPAD * (NPAD + 1) / 2;
   __shared__ TargetSmem<NPAD> ts;
   __shared__ double Kp[NK];                 // K64 packed lower (row-major)
-  __shared__ T cb[2][NPAD + MAXC + 2];      // column broadcast (double-buffered)
+  __shared__ __align__(16) T cb[2][NPAD + 16];  // column broadcast (double-buffered)
   __shared__ double cols[MAXC][NPAD];       // forward-substituted columns / W
   __shared__ double wvec[REFINE ? MAXC : 1][NPAD];  // raw F | k | u columns (refinement)
   __shared__ double G[MAXC * MAXC];

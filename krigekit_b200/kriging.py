@@ -95,6 +95,7 @@ class Kriging:
         _lib.check(lib.krige_create(ctypes.byref(h)), "krige_create")
         self._handle = h.value
         self._lib = lib
+        _lib.register(self)
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
         _lib.call("krige_set_device", self._h(), dev, ctypes.c_void_p(stream))
@@ -125,12 +126,18 @@ class Kriging:
     def _h(self):
         return ctypes.c_int64(self._handle)
 
+    def close(self):
+        """Release the handle and its device buffers (krige_destroy)."""
+        if getattr(self, "_handle", 0):
+            h = ctypes.c_int64(self._handle)
+            self._handle = 0
+            self._lib.krige_destroy(ctypes.byref(h))
+
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
-            if getattr(self, "_handle", 0):
-                h = ctypes.c_int64(self._handle)
-                self._lib.krige_destroy(ctypes.byref(h))
-                self._handle = 0
+            self.close()
         except Exception:
             pass
 
@@ -271,6 +278,18 @@ class Kriging:
         _lib.call("krige_gpu_stats", self._h(), buf, ctypes.byref(ms))
         return {"fail": buf[0], "chol": buf[1], "ldlt": buf[3], "search_redo": buf[5],
                 "fp64_resolve": buf[6], "refine_iterations": buf[7], "solve_ms": ms.value}
+
+    def profile(self, enable: bool = True):
+        """Record per-phase device time of each solve (extension)."""
+        _lib.call("krige_gpu_profile", self._h(), int(bool(enable)))
+
+    def phases(self) -> dict:
+        """Device ms per phase of the last solve and its kernel launches (extension)."""
+        out = (ctypes.c_double * 4)()
+        nl = ctypes.c_int(0)
+        _lib.call("krige_gpu_phases", self._h(), out, ctypes.byref(nl))
+        return {"search_ms": out[0], "bucket_ms": out[1], "solve_ms": out[2], "fallback_ms": out[3],
+                "launches": nl.value}
 
     # ------------------------------------------------------------------ results
     def _nb(self):
