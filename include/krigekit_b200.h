@@ -120,6 +120,20 @@ int krige_gpu_profile(int64_t handle, int enable);
  * launches = kernels launched by that solve. */
 int krige_gpu_phases(int64_t handle, double *out4, int *launches);
 
+/* No counterpart in the reference.  Allocation-free FP64 re-solve: repeats the
+ * last krige_solve of this handle with the same neighbour sets, after replacing
+ * the observation values of variable ivar with value[nobs] (value may be NULL
+ * to keep them).  It allocates no device memory: the one-thread-per-target
+ * kernel runs with its workspace, work list and counters in a fixed 32 MiB
+ * static device array.  A system whose workspace exceeds that array (about
+ * 1440 equations for one variable) is rejected with an error.  Needs a
+ * completed krige_solve with no set_obs / set_grid / set_search since.  The
+ * first call on a device looks up the array's address and belongs before any
+ * stream capture on that device.  Calls on one device share the array and are
+ * serialised inside the library; the call returns after its work has finished.
+ * Results are read with the usual getters. */
+int krige_resolve_static(int64_t handle, int ivar, int nobs, const double *value);
+
 #ifdef __cplusplus
 }
 #endif

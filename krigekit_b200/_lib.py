@@ -82,6 +82,7 @@ SIGNATURES = {
     "krige_gpu_stats": ([_c_i64, _p_int, _p_dbl], _c_int),
     "krige_gpu_profile": ([_c_i64, _c_int], _c_int),
     "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),
+    "krige_resolve_static": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
 }
 
 _lib = None

@@ -629,4 +629,15 @@ int krige_gpu_phases(int64_t h, double* out4, int* launches) {
   KK_GUARD_END
 }
 
+// Allocation-free FP64 re-solve of the last krige_solve's neighbour sets
+// (no counterpart in the reference): for callers that must not have device
+// memory allocated during the call.  value may be null.
+int krige_resolve_static(int64_t h, int ivar, int nobs, const double* value) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_resolve_static(*e, ivar, nobs, value);
+  KK_GUARD_END
+}
+
 }  // extern "C"

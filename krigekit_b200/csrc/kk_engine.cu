@@ -298,6 +298,62 @@ struct PhaseTimer {
   }
 };
 
+// Solve parameters from the engine's device buffers (after the search).
+static void fill_params(Engine& e, SolveParams& P) {
+  const int nv = e.nvar, nb = e.nblock;
+  std::memset(&P, 0, sizeof P);
+  P.nvar = nv;
+  P.ndim = e.ndim;
+  P.nlag = e.nlag;
+  P.st = e.st;
+  P.ndrift = e.ndrift;
+  P.naug = e.naug();
+  P.pa = e.pdrift();
+  P.std_ck = e.std_ck;
+  P.unbias = e.unbias;
+  P.ck_isa = (!e.std_ck && e.unbias != 0 && nv > 1) ? 1 : 0;
+  P.sk_any = 0;
+  for (int v = 0; v < nv; ++v) {
+    P.sk_mean[v] = e.obs[v].sk_mean;
+    if (e.unbias == 0 && e.obs[v].sk_mean != 0.0) P.sk_any = 1;
+  }
+  P.nmin = e.nmin;
+  P.neglect_error = e.neglect_error;
+  P.bounds[0] = e.bounds[0];
+  P.bounds[1] = e.bounds[1];
+  P.models = e.st ? nullptr : e.models.as<KkModel>();
+  P.smodels = e.st ? e.models.as<KkSTModel>() : nullptr;
+  P.tables = e.tables.as<double2>();
+  for (int v = 0; v < nv; ++v) {
+    VarDevice& d = e.vd[v];
+    for (int k = 0; k < 4; ++k) P.ox[v][k] = d.x[k].as<double>();
+    P.oval[v] = d.value.as<double>();
+    P.ovar[v] = d.variance.as<double>();
+    P.odrift[v] = d.drift.as<double>();
+    P.nobs[v] = e.obs[v].n;
+    P.nbr[v] = d.nbr.as<int>();
+    P.nnear[v] = d.nnear.as<int>();
+    P.mmax[v] = std::max(d.search.mmax, 1);
+  }
+  P.nblock = nb;
+  for (int k = 0; k < 4; ++k) P.tx[k] = e.tx[k].as<double>();
+  P.rs = e.rangescale.empty() ? nullptr : e.trs.as<double>();
+  P.ln = e.localnugget.empty() ? nullptr : e.tln.as<double>();
+  P.tdrift = e.ndrift > 0 ? e.tdrift.as<double>() : nullptr;
+  P.gstart = e.nblockpnt.empty() ? nullptr : e.gstart.as<int>();
+  for (int k = 0; k < 4; ++k) P.gx[k] = e.nblockpnt.empty() ? nullptr : e.gx[k].as<double>();
+  P.gw = e.nblockpnt.empty() ? nullptr : e.gw.as<double>();
+  P.est = e.est.as<double>();
+  P.var = e.var.as<double>();
+  P.status = e.status.as<int>();
+  P.counters = e.counters.as<int>();
+  P.fb_list = e.npp.as<int>();
+  P.fp64_list = e.npp.as<int>() + nb;
+  P.refine_tol = 1.0e-10;
+  if (P.pa + nv + 1 + ((P.ck_isa || P.sk_any) ? nv : 0) > 8)
+    throw std::string("too many drift/variable columns for the register kernels (max 8)");
+}
+
 void engine_solve(Engine& e) {
   auto t0 = std::chrono::steady_clock::now();
   for (double& x : e.phase_ms) x = 0.0;
@@ -442,57 +498,7 @@ void engine_solve(Engine& e) {
 
   // ---- solve parameters
   SolveParams P;
-  std::memset(&P, 0, sizeof P);
-  P.nvar = nv;
-  P.ndim = e.ndim;
-  P.nlag = e.nlag;
-  P.st = e.st;
-  P.ndrift = e.ndrift;
-  P.naug = e.naug();
-  P.pa = e.pdrift();
-  P.std_ck = e.std_ck;
-  P.unbias = e.unbias;
-  P.ck_isa = (!e.std_ck && e.unbias != 0 && nv > 1) ? 1 : 0;
-  P.sk_any = 0;
-  for (int v = 0; v < nv; ++v) {
-    P.sk_mean[v] = e.obs[v].sk_mean;
-    if (e.unbias == 0 && e.obs[v].sk_mean != 0.0) P.sk_any = 1;
-  }
-  P.nmin = e.nmin;
-  P.neglect_error = e.neglect_error;
-  P.bounds[0] = e.bounds[0];
-  P.bounds[1] = e.bounds[1];
-  P.models = e.st ? nullptr : e.models.as<KkModel>();
-  P.smodels = e.st ? e.models.as<KkSTModel>() : nullptr;
-  P.tables = e.tables.as<double2>();
-  for (int v = 0; v < nv; ++v) {
-    VarDevice& d = e.vd[v];
-    for (int k = 0; k < 4; ++k) P.ox[v][k] = d.x[k].as<double>();
-    P.oval[v] = d.value.as<double>();
-    P.ovar[v] = d.variance.as<double>();
-    P.odrift[v] = d.drift.as<double>();
-    P.nobs[v] = e.obs[v].n;
-    P.nbr[v] = d.nbr.as<int>();
-    P.nnear[v] = d.nnear.as<int>();
-    P.mmax[v] = std::max(d.search.mmax, 1);
-  }
-  P.nblock = nb;
-  for (int k = 0; k < 4; ++k) P.tx[k] = e.tx[k].as<double>();
-  P.rs = e.rangescale.empty() ? nullptr : e.trs.as<double>();
-  P.ln = e.localnugget.empty() ? nullptr : e.tln.as<double>();
-  P.tdrift = e.ndrift > 0 ? e.tdrift.as<double>() : nullptr;
-  P.gstart = e.nblockpnt.empty() ? nullptr : e.gstart.as<int>();
-  for (int k = 0; k < 4; ++k) P.gx[k] = e.nblockpnt.empty() ? nullptr : e.gx[k].as<double>();
-  P.gw = e.nblockpnt.empty() ? nullptr : e.gw.as<double>();
-  P.est = e.est.as<double>();
-  P.var = e.var.as<double>();
-  P.status = e.status.as<int>();
-  P.counters = e.counters.as<int>();
-  P.fb_list = e.npp.as<int>();
-  P.fp64_list = e.npp.as<int>() + nb;
-  P.refine_tol = 1.0e-10;
-  if (P.pa + nv + 1 + ((P.ck_isa || P.sk_any) ? nv : 0) > 8)
-    throw std::string("too many drift/variable columns for the register kernels (max 8)");
+  fill_params(e, P);
 
   // ---- bucket + solve
   timer.start();
@@ -549,6 +555,56 @@ void engine_solve(Engine& e) {
   if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");
   e.solved = true;
   e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value) {
+  // Everything below works in buffers the last krige_solve left behind: no
+  // DBuf::reserve, no allocator callback, no cudaMalloc.
+  if (!e.solved) throw std::string("krige_resolve_static needs a completed krige_solve on this handle");
+  if (e.grid_dirty) throw std::string("targets changed since the last krige_solve; call krige_solve");
+  for (int v = 0; v < e.nvar; ++v)
+    if (e.obs[v].dirty || e.obs[v].search_dirty)
+      throw std::string("observations or search changed since the last krige_solve; call krige_solve");
+  if (value) {
+    if (ivar < 1 || ivar > e.nvar) throw std::string("ivar out of range");
+    if (nobs != e.obs[ivar - 1].n) throw std::string("size(value) /= obs%n");
+  }
+  KK_CUDA(cudaSetDevice(e.device));
+  cudaStream_t st = e.stream;
+  // the variogram may have been reset since the last solve: rebuild the
+  // models on the host and copy them into the existing buffers when they fit
+  std::vector<KkModel> mdl;
+  std::vector<KkSTModel> smdl;
+  std::vector<double2> tabs;
+  build_models(e, mdl, smdl, tabs);
+  if (tabs.empty()) tabs.push_back(make_double2(0.0, 0.0));
+  const size_t tb = sizeof(double2) * tabs.size();
+  const size_t mb = e.st ? sizeof(KkSTModel) * smdl.size() : sizeof(KkModel) * mdl.size();
+  if (tb > e.tables.bytes || mb > e.models.bytes)
+    throw std::string("the variogram tables outgrew the buffers of the last krige_solve; call krige_solve");
+  e.solved = false;
+  set_zones(st);
+  KK_CUDA(cudaMemcpyAsync(e.tables.p, tabs.data(), tb, cudaMemcpyHostToDevice, st));
+  KK_CUDA(cudaMemcpyAsync(e.models.p, e.st ? (const void*)smdl.data() : (const void*)mdl.data(), mb,
+                          cudaMemcpyHostToDevice, st));
+  if (value) {
+    ObsVar& o = e.obs[ivar - 1];
+    std::copy(value, value + nobs, o.value.begin());
+    KK_CUDA(cudaMemcpyAsync(e.vd[ivar - 1].value.p, o.value.data(), sizeof(double) * nobs,
+                            cudaMemcpyHostToDevice, st));
+  }
+  SolveParams P;
+  fill_params(e, P);
+  int cnt[KK_CNT_N];
+  solve_generic_static(P, e.device, st, e.mmax_total + P.pa, cnt);
+  std::memset(e.stats, 0, sizeof e.stats);
+  e.stats[0] = cnt[KK_CNT_FAIL];
+  e.stats[1] = cnt[KK_CNT_CHOL];
+  e.stats[3] = cnt[KK_CNT_LDLT];
+  for (double& x : e.phase_ms) x = 0.0;
+  e.launches = 2 * ((e.nblock + KK_STATIC_CHUNK - 1) / KK_STATIC_CHUNK);
+  if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");
+  e.solved = true;
 }
 
 void engine_release(Engine& e) {

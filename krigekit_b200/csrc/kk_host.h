@@ -117,6 +117,10 @@ void build_kdtree(const double* data, int D, int n, std::vector<int>& node_i,
 
 // engine entry points (kk_engine.cu)
 void engine_solve(Engine& e);
+// FP64 re-solve of the last solve's neighbour sets without any device
+// allocation (workspace in a fixed static array); value (nobs) replaces the
+// observation values of variable ivar first when it is not null.
+void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value);
 void engine_release(Engine& e);
 
 // allocator hook

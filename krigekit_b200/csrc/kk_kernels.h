@@ -81,4 +81,22 @@ void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st);
 void set_zones(cudaStream_t st);
 
+// Doubles of generic-kernel workspace per thread for systems of at most mtot
+// equations (neighbours + drift/unbiasedness rows) with nv right-hand sides
+// and pa drift/unbiasedness rows.
+inline size_t generic_stride(int mtot, int nv, int pa) {
+  return (size_t)mtot * mtot * 2 + (size_t)nv * mtot * 3 + (size_t)mtot * (pa + 2) + (size_t)(pa + 1) * (pa + 1) +
+         (size_t)(pa + 1) * nv + (size_t)mtot + 64;
+}
+
+// Size of the fixed device array behind solve_generic_static (per device).
+constexpr size_t KK_STATIC_SCRATCH_BYTES = (size_t)32 << 20;
+constexpr int KK_STATIC_CHUNK = 1 << 16;  // targets per work-list chunk (two launches each)
+
+// FP64 re-solve of every target through the generic kernel with workspace,
+// work list and counters in the fixed static array instead of engine
+// buffers; copies the counters of the run into cnt[KK_CNT_N] and
+// synchronises st.  The caller has made `device` current.
+void solve_generic_static(SolveParams P, int device, cudaStream_t st, int mtot, int* cnt);
+
 }  // namespace kk

@@ -21,6 +21,11 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
 #include "kk_device.cuh"
 #include "kk_kernels.h"
 
@@ -1017,6 +1022,97 @@ void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st) {
   int blocks = (nthreads + 63) / 64;
   k_solve_generic<<<blocks, 64, 0, st>>>(P, list, P.counters + list_cnt_slot);
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free re-solve: the generic kernel on a fixed static array
+// ---------------------------------------------------------------------------
+// Some callers cannot let the library allocate device memory in the middle of
+// a call.  A serving loop that keeps other streams busy would be stalled,
+// because cudaMalloc and cudaFree may synchronise the whole device; a process
+// whose HBM is already reserved by another allocator's pool would see the
+// allocation fail, or force that pool to give back its cached blocks.  For
+// those callers krige_resolve_static runs k_solve_generic with its workspace,
+// its work list and its counters in this one array, sized once when the
+// module is loaded.  The array exists once per device and per process, so
+// calls on one device must not overlap in time: solve_generic_static holds a
+// process-wide lock until the call's work on the device has finished.
+constexpr size_t KK_STATIC_HEADER = 256;      // counters (KK_CNT_N ints), then the list count
+constexpr size_t KK_STATIC_LIST_BYTES = sizeof(int) * KK_STATIC_CHUNK;
+static __device__ __align__(256) unsigned char g_static_scratch[KK_STATIC_SCRATCH_BYTES];
+
+static std::mutex g_static_mu;
+static void* g_static_addr[64];
+
+// Work list of the targets t0 <= t < t1 that have a solvable neighbour set;
+// the others get NaN exactly as in k_bucket.  Status bits of the previous
+// solve are cleared except those the search set.
+__global__ void k_static_list(SolveParams P, int t0, int t1, int* __restrict__ list, int* __restrict__ count) {
+  const int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= t1) return;
+  int npp = 0;
+  for (int v = 0; v < P.nvar; ++v) npp += P.nnear[v][t];
+  P.status[t] &= (KK_ST_TIE | KK_ST_OVERFLOW);
+  if (npp == 0 || npp == 1 || (P.nmin > 0 && npp < P.nmin)) {
+    write_nan(P, t);
+    P.status[t] |= KK_ST_EMPTY;
+    if (npp == 0 && !P.neglect_error) atomicAdd(&P.counters[KK_CNT_FAIL], 1);
+    return;
+  }
+  list[atomicAdd(count, 1)] = t;
+}
+
+static void static_check(cudaError_t err, const char* what) {
+  if (err != cudaSuccess) throw std::string("CUDA error ") + cudaGetErrorString(err) + " at " + what;
+}
+
+void solve_generic_static(SolveParams P, int device, cudaStream_t st, int mtot, int* cnt) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (device < 0 || device >= 64) throw std::string("device ordinal out of range for the static scratch");
+  if (!g_static_addr[device]) {
+    // Set-up, once per device with that device current: the address of this
+    // device's copy of the array.  It may load the module, so the first call
+    // on a device belongs before any stream capture on it.
+    void* addr = nullptr;
+    static_check(cudaGetSymbolAddress(&addr, g_static_scratch), "cudaGetSymbolAddress(g_static_scratch)");
+    g_static_addr[device] = addr;
+  }
+  unsigned char* base = static_cast<unsigned char*>(g_static_addr[device]);
+  const size_t ws_bytes = KK_STATIC_SCRATCH_BYTES - KK_STATIC_HEADER - KK_STATIC_LIST_BYTES;
+  const size_t stride = generic_stride(mtot, P.nvar, P.pa);
+  const size_t slots = ws_bytes / (stride * sizeof(double));
+  if (slots < 1) {
+    char msg[256];
+    snprintf(msg, sizeof msg,
+             "krige_resolve_static: one target needs %zu bytes of workspace (%d equations), more than the %zu "
+             "bytes of static scratch; use krige_solve",
+             stride * sizeof(double), mtot, ws_bytes);
+    throw std::string(msg);
+  }
+  int* counters = reinterpret_cast<int*>(base);
+  int* list_count = counters + KK_CNT_N;
+  int* list = reinterpret_cast<int*>(base + KK_STATIC_HEADER);
+  P.counters = counters;
+  P.fb_list = nullptr;
+  P.fp64_list = nullptr;
+  P.scratch = reinterpret_cast<double*>(base + KK_STATIC_HEADER + KK_STATIC_LIST_BYTES);
+  P.scratch_stride = (int)stride;
+  // thread g of the generic kernel owns workspace slot g: never more threads than slots
+  const int threads = (int)std::min<size_t>(slots, (size_t)KK_STATIC_CHUNK);
+  const int bs = std::min(64, threads);
+  const int blocks = threads / bs;
+  // the counters and the list count start at zero
+  static_check(cudaMemsetAsync(base, 0, KK_STATIC_HEADER, st), "cudaMemsetAsync(static header)");
+  for (int t0 = 0; t0 < P.nblock; t0 += KK_STATIC_CHUNK) {
+    const int t1 = std::min(P.nblock, t0 + KK_STATIC_CHUNK);
+    static_check(cudaMemsetAsync(list_count, 0, sizeof(int), st), "cudaMemsetAsync(static list count)");
+    k_static_list<<<(t1 - t0 + 255) / 256, 256, 0, st>>>(P, t0, t1, list, list_count);
+    k_solve_generic<<<blocks, bs, 0, st>>>(P, list, list_count);
+    static_check(cudaGetLastError(), "k_solve_generic (static scratch)");
+  }
+  static_check(cudaMemcpyAsync(cnt, counters, sizeof(int) * KK_CNT_N, cudaMemcpyDeviceToHost, st),
+               "cudaMemcpyAsync(static counters)");
+  static_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
 }
 
 }  // namespace kk

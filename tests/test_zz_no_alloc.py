@@ -1,0 +1,126 @@
+"""krige_resolve_static: the allocation-free FP64 re-solve, through the C-ABI.
+
+It re-solves the neighbour sets of the last krige_solve with the generic
+one-thread-per-target kernel whose workspace, work list and counters live in
+a fixed static device array.  Each case calls it twice in a row with new
+observation values and compares both results with the existing entry points
+(krige_update_obs_value + krige_solve in FP64) on a second handle, and
+checks that the torch caching allocator saw no allocation during the calls.
+This file is collected last so that it also runs after every other GPU test.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import bench_workloads as bw
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-9
+
+
+def _handle_pair(w):
+    from krigekit_b200 import Kriging
+    kw = dict(ndim=w["ndim"], nvar=w["nvar"], **w["kw"])
+    a = bw.apply(Kriging(precision="fp64", **kw), w)
+    b = bw.apply(Kriging(precision="fp64", **kw), w)
+    return a, b
+
+
+def _results(k):
+    e, v = k.get_results(squeeze=False)
+    return np.array(e), np.array(v)
+
+
+def _resolve_static(k, ivar, value):
+    from krigekit_b200 import _lib
+    lib = _lib.load()
+    if value is None:
+        ierr = lib.krige_resolve_static(ctypes.c_int64(k._handle), 0, 0, None)
+    else:
+        v = np.ascontiguousarray(value, dtype=np.float64)
+        ierr = lib.krige_resolve_static(ctypes.c_int64(k._handle), ivar, v.size,
+                                        v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return int(ierr)
+
+
+def _allocations():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.memory_stats().get("allocation.all.allocated", 0)
+
+
+def _check_two_calls(w, ivar):
+    from krigekit_b200 import _lib
+    a, b = _handle_pair(w)
+    a.solve()
+    b.solve()
+    z0 = np.asarray(w["obs"][ivar - 1]["value"], dtype=np.float64)
+    rng = np.random.default_rng(77)
+    for call in range(2):
+        znew = z0 * (1.0 + 0.5 * call) + rng.normal(0.0, 0.1, z0.size)
+        before = _allocations()
+        ierr = _resolve_static(a, ivar, znew)
+        after = _allocations()
+        assert ierr == 0, _lib.last_error()
+        assert after == before, f"call {call}: {after - before} device allocations"
+        b.update_obs_value(ivar, znew)
+        b.solve()
+        e_s, v_s = _results(a)
+        e_r, v_r = _results(b)
+        assert np.array_equal(np.isnan(e_s), np.isnan(e_r))
+        ok = ~np.isnan(e_r)
+        zstd = float(np.std(znew))
+        ee = bw.rel_err(e_s[ok], e_r[ok], 1e-3 * zstd)
+        ve = bw.rel_err(v_s, v_r, 1e-3 * w["sill"])
+        assert np.nanmax(ee) <= TOL, f"call {call}: estimate rel err {np.nanmax(ee):.3e}"
+        assert np.nanmax(ve) <= TOL, f"call {call}: variance rel err {np.nanmax(ve):.3e}"
+        assert a.solver_stats["fail"] == 0
+    # null values: the same neighbour sets and values give the same results again
+    e1, v1 = _results(a)
+    assert _resolve_static(a, 0, None) == 0, _lib.last_error()
+    e2, v2 = _results(a)
+    np.testing.assert_array_equal(e1, e2)
+    np.testing.assert_array_equal(v1, v2)
+    a.close()
+    b.close()
+
+
+def test_resolve_static_sector_search():
+    w = bw.config2(grid_n=70, nobs=6000, nclusters=12)
+    _check_two_calls(w, 1)
+
+
+def test_resolve_static_cokriging():
+    w = bw.config4(grid_n=40, nobs=(600, 4000))
+    _check_two_calls(w, 2)
+
+
+def test_resolve_static_rejects_oversized_systems():
+    from krigekit_b200 import Kriging, _lib
+    rng = np.random.default_rng(5)
+    n = 1500  # one system of 1501 equations needs ~36 MB of workspace, above the 32 MiB array
+    obs = rng.uniform(0, 1, (n, 2))
+    k = Kriging(precision="fp64")
+    k.set_obs(1, obs, np.sin(6 * obs[:, 0]), nmax=n)
+    k.set_vgm(1, 1, "exp", nugget=0.1, sill=1.0, a_major=0.3)
+    k.set_grid(np.array([[0.5, 0.5]]))
+    k.set_search(1)
+    k.solve()
+    assert _resolve_static(k, 0, None) == 1
+    assert "static scratch" in _lib.last_error()
+    k.close()
+
+
+def test_resolve_static_needs_a_solve():
+    from krigekit_b200 import Kriging, _lib
+    w = bw.config1(grid_n=10, nobs=200)
+    k = bw.apply(Kriging(precision="fp64", ndim=2, nvar=1), w)
+    assert _resolve_static(k, 0, None) == 1
+    assert "krige_solve" in _lib.last_error()
+    k.solve()
+    k.set_obs(1, w["obs"][0]["coord"], w["obs"][0]["value"], nmax=32)
+    assert _resolve_static(k, 0, None) == 1
+    assert "krige_solve" in _lib.last_error()
+    k.close()
