@@ -105,6 +105,7 @@ __global__ void k_bucket(SolveParams P, int* __restrict__ lists) {
     return;
   }
   slot = npp <= 32 ? KK_CNT_B16 : (npp <= 64 ? KK_CNT_B64 : KK_CNT_BIG);
+  if (slot == KK_CNT_BIG) P.status[t] |= KK_ST_BIG;
   int p = atomicAdd(&P.counters[slot], 1);
   lists[(size_t)slot * P.nblock + p] = t;
 }
@@ -274,6 +275,34 @@ __device__ __noinline__ void finish_outputs(const SolveParams& P, int t, const d
     }
   }
 }
+
+// Covariance of one neighbour row (coordinates xr, variable vr) with the
+// target for target variable iv, averaged over block nodes (assemble_rhs,
+// kriging.F90:889-910).
+__device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const double* xr, int vr, int iv, double rs) {
+  double tmp = 0.0;
+  if (P.gstart) {
+    const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
+    for (int k = k0; k < k1; ++k) {
+      double node[4], lag[4];
+      for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
+      make_lag(P, xr, node, rs, lag);
+      tmp = dadd(tmp, dmul(cov_pair(P, vr, iv, lag), __ldg(&P.gw[k])));
+    }
+  } else {
+    double node[4], lag[4];
+    for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
+    make_lag(P, xr, node, rs, lag);
+    tmp = dadd(tmp, dmul(cov_pair(P, vr, iv, lag), 1.0));
+  }
+  return tmp;
+}
+
+}  // namespace kk
+
+#include "kk_warp.cuh"
+
+namespace kk {
 
 // ---------------------------------------------------------------------------
 // register kernel: one CTA of NPAD threads per target, thread i owns row i
@@ -1000,23 +1029,38 @@ static void launch_reg(const SolveParams& P, const int* list, const int* cnt, in
   k_solve_reg<T, NPAD, REFINE><<<nsm * occ, NPAD, 0, st>>>(P, list, cnt, slot);
 }
 
+template <typename T, int N, bool REFINE>
+static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int slot, int nsm, cudaStream_t st) {
+  constexpr int WPC = warp_cta<T, N, REFINE>();
+  const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
+  static bool attr_set = false;  // per instantiation
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE>, 32 * WPC, smem);
+  if (occ < 1) occ = 1;
+  k_solve_warp<T, N, REFINE><<<nsm * occ, 32 * WPC, smem, st>>>(P, list, cnt, slot);
+}
+
 void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm, cudaStream_t st) {
   const int* c = P.counters;
   const int* l32 = lists + (size_t)KK_CNT_B16 * P.nblock;
   const int* l64 = lists + (size_t)KK_CNT_B64 * P.nblock;
-  if (precision == 0) {
-    launch_reg<double, 32, false>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
-    launch_reg<double, 64, false>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
+  if (precision == 0 || P.pa + P.nvar > KK_REFINE_COLS) {
+    launch_warp<double, 32, false>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
+    launch_warp<double, 64, false>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
   } else {
-    launch_reg<float, 32, true>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
-    launch_reg<float, 64, true>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
+    launch_warp<float, 32, true>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
+    launch_warp<float, 64, true>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
   }
 }
 
-// FP64 register solve of an explicit list (FP32 non-convergence fallback):
-// the list is split by size inside the kernel via the padding bound
+// FP64 solve of an explicit list of targets with at most 64 neighbours (FP32
+// refinement that did not converge, or an FP32 factorisation that failed)
 void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_slot, int nsm, cudaStream_t st) {
-  launch_reg<double, 64, false>(P, list, P.counters + list_cnt_slot, KK_CNT_WORK0 + 2, nsm, st);
+  launch_warp<double, 64, false>(P, list, P.counters + list_cnt_slot, KK_CNT_WORK0 + 2, nsm, st);
 }
 
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st) {

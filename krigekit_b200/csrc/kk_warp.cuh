@@ -1,0 +1,612 @@
+// kk_warp.cuh -- warp-per-target kriging solve (included by kk_solve.cu).
+//
+// One warp owns one target system at a time and pulls the next target from
+// a device work counter, so the solve needs no block-wide barrier at all.
+//
+// Register layout of the N x N covariance matrix K (N = 32 or 64): the warp
+// is a 4 x 8 grid of lanes, pr = lane & 3 (row class), pc = lane >> 2
+// (column class).  Lane (pr, pc) owns entry (r, c) = (4 ri + pr, 8 ci + pc)
+// in register slot a[ri][ci]; only slots with ri >= 2 ci can hold lower-
+// triangle entries, so a lane keeps 72 slots for N = 64 (20 for N = 32) and
+// the trailing update of every Cholesky column is spread evenly over the
+// 32 lanes.  Right-hand-side rows are owned one per (lane, m):
+// r = 32 m + 4 pc + pr.
+//
+// Per target:
+//   1. gather the neighbour rows (ascending index per variable block, as
+//      assemble_linear_system_base, kriging_base.F90:3159-3235);
+//   2. every lane evaluates its own K entries (assemble_lhs, kriging.F90:
+//      714-849) and its right-hand-side rows F | k | u (assemble_rhs,
+//      kriging.F90:864-939) -- no shared-memory round trip;
+//   3. right-looking Cholesky, one __syncwarp per column: the lanes of
+//      column class j % 8 publish column j of L to shared memory, every lane
+//      applies the rank-1 update to its slots and forward-substitutes its
+//      right-hand-side rows in the same sweep;
+//   4. FP64: the outputs are inner products of forward-substituted columns
+//      (S = F^T K^-1 F, lambda, variance, estimate); FP32 + refinement: the
+//      FP32 factor is kept packed in shared memory, the solution of
+//      K [W] = [F k] is refined with FP64 residuals against K64 (also kept in
+//      shared memory) until the estimated error is below refine_tol; then
+//      the same inner products are taken against the refined W.
+#pragma once
+
+// right-hand-side columns solved by the refinement form (F and k: pa + nvar);
+// systems with more columns are solved by the FP64 form
+#define KK_REFINE_COLS 4
+
+namespace kk {
+
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return 1.0 / sqrt(x); }
+
+// zone constants of the lookup tables, held in registers
+struct ZoneRegs {
+  double zb1, zb2, zb3, i0, i1, i2;
+  int o1, o2, n0, n1, n2;
+};
+
+__device__ __forceinline__ ZoneRegs load_zones() {
+  ZoneRegs z;
+  z.zb1 = c_zones.zb[1];
+  z.zb2 = c_zones.zb[2];
+  z.zb3 = c_zones.zb[3];
+  z.i0 = c_zones.inv_dh[0];
+  z.i1 = c_zones.inv_dh[1];
+  z.i2 = c_zones.inv_dh[2];
+  z.o1 = c_zones.off[1];
+  z.o2 = c_zones.off[2];
+  z.n0 = c_zones.zn[0];
+  z.n1 = c_zones.zn[1];
+  z.n2 = c_zones.zn[2];
+  return z;
+}
+
+// tab_lookup without divergent constant-memory indexing: the same zone
+// choice, index and interpolation (variogram.f90:353-382, 682-710) from
+// register selects.  Valid for 0 <= h < zb3.
+__device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, const ZoneRegs& z, double h) {
+  const bool z0 = h < z.zb1, z1 = h < z.zb2;
+  const double lo = z0 ? 0.0 : (z1 ? z.zb1 : z.zb2);
+  const double inv = z0 ? z.i0 : (z1 ? z.i1 : z.i2);
+  const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
+  const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
+  double fi = dmul(dsub(h, lo), inv);
+  const int ii = (int)fi;
+  const int i = off + min(ii, nm1);
+  fi = dsub(fi, (double)ii);
+  const double2 t = __ldg(&tab[i]);
+  return dadd(t.x, dmul(fi, t.y));
+}
+
+// One Level-B model held in registers (single-variable spatial kriging):
+// COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past the table.
+struct FastModel {
+  double m[9];
+  const double2* tab;
+  const KkModel* model;
+  int ndim, tail;
+};
+
+// analytic tail past the last table zone (struct_cov_h), kept out of line so
+// that the rarely taken shape code does not raise the kernel's register count
+__device__ __noinline__ double tail_cov(const KkModel* m, double h) { return model_cov_h(*m, h); }
+
+// COV(vgm(first, second), lag) for models without a register fast path
+__device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, int second, const double* lag) {
+  return cov_pair(P, first, second, lag);
+}
+
+__device__ __forceinline__ double fast_cov(const FastModel& f, const ZoneRegs& z, const double* lag) {
+  const double h = aniso_h(f.m, f.ndim, lag);
+  if (h < z.zb3) return tab_fast(f.tab, z, h);
+  return f.tail ? tail_cov(f.model, h) : 0.0;
+}
+
+template <typename T, int N, bool REFINE>
+struct __align__(16) WarpSmem {
+  double x[4][N];          // neighbour coordinates (nlag)
+  double z[N];             // neighbour values
+  int obs[N];
+  int var[N];
+  T col[2][N];             // column j of L, layout [pr][ri]
+  double ybc[2][MAXC];     // forward-substituted right-hand sides of row j
+  double G[MAXC * MAXC];
+  double zmean[2 * KK_MAXVAR];
+  double K[N * (N + 1) / 2];               // K64 packed row-major lower
+  float L[REFINE ? N * (N - 1) / 2 : 1];   // FP32 factor, strictly lower, packed by column
+  float invd[REFINE ? N : 1];              // 1 / L[j][j]
+  double W[REFINE ? KK_REFINE_COLS * N : 1];         // current solution, broadcast for the residual
+};
+
+// start of column c of the strictly-lower packed factor
+template <int N>
+__device__ __forceinline__ int lcol(int c) { return c * (N - 1) - (c * (c - 1)) / 2; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// warps per CTA: the FP32 + refinement form at N = 64 keeps K64 and L in
+// shared memory (about 33 KB per warp), so it runs two warps per CTA
+template <typename T, int N, bool REFINE>
+constexpr int warp_cta() { return (REFINE && N == 64) ? 2 : 4; }
+
+// CTAs per SM the register budget is sized for (the launch bound caps the
+// registers at 64 K / (threads * this)): the N = 64 forms need the whole
+// register file of a lane for the matrix, the N = 32 forms fit in 128
+template <typename T, int N, bool REFINE>
+constexpr int warp_min_ctas() { return N == 64 ? 1 : 4; }
+
+template <typename T, int N, bool REFINE>
+__global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE>())
+    k_solve_warp(const __grid_constant__ SolveParams P, const int* __restrict__ list,
+                 const int* __restrict__ list_count, int work_slot) {
+  using WS = WarpSmem<T, N, REFINE>;
+  constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
+  constexpr int CB = REFINE ? KK_REFINE_COLS : MAXC;  // right-hand-side columns held per row
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WS& s = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int pr = lane & 3, pc = lane >> 2;
+  const int n_items = *list_count;
+  const int q = P.nvar, pa = P.pa;
+  const int nu = n_func(P);
+  const int C = pa + q + nu;  // forward-substituted columns (FP64 form)
+  const int nc = pa + q;      // solved columns (refinement form)
+  const int ncols = REFINE ? nc : C;
+  const ZoneRegs zr = load_zones();
+
+  FastModel fm;
+  const bool fast = !P.st && q == 1 && P.models[0].mode == KK_LEVEL_B;
+  if (fast) {
+    const KkModel& m0 = P.models[0];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fm.m[k] = m0.bmat[k];
+    fm.tab = P.tables + m0.btab_off;
+    fm.model = &m0;
+    fm.ndim = m0.ndim;
+    fm.tail = m0.btail;
+  }
+
+  int n_chol = 0, n_iter = 0;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(&P.counters[work_slot], 1);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= n_items) break;
+    const int t = __ldg(&list[item]);
+
+    // ---- neighbour rows: variable blocks in order, ascending index
+    int ist1 = 0x7fffffff, ist2 = 0x7fffffff, ist3 = 0x7fffffff, n = 0;
+#pragma unroll
+    for (int v = 0; v < KK_MAXVAR; ++v) {
+      if (v < q) {
+        if (v == 1) ist1 = n;
+        if (v == 2) ist2 = n;
+        if (v == 3) ist3 = n;
+        n += __ldg(&P.nnear[v][t]);
+      }
+    }
+    const double rs = P.rs ? __ldg(&P.rs[t]) : 1.0;
+    const double ln = P.ln ? __ldg(&P.ln[t]) : 0.0;
+    for (int r = lane; r < n; r += 32) {
+      const int v = (r >= ist1) + (r >= ist2) + (r >= ist3);
+      const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
+      const int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (r - i0)]);
+      s.obs[r] = o;
+      s.var[r] = v;
+      for (int d = 0; d < P.nlag; ++d) s.x[d][r] = __ldg(&P.ox[v][d][o]);
+      s.z[r] = __ldg(&P.oval[v][o]);
+    }
+    __syncwarp();
+    const int nri = (n + 3) >> 2, nci = (n + 7) >> 3;
+
+    // ---- right-hand-side rows r = 32 m + 4 pc + pr: F (pa), k (q), u (nu)
+    T b[RM][CB];
+    double b64[REFINE ? RM : 1][REFINE ? CB : 1];
+#pragma unroll
+    for (int m = 0; m < RM; ++m) {
+      const int r = 32 * m + 4 * pc + pr;
+#pragma unroll
+      for (int k = 0; k < CB; ++k) b[m][k] = T(0);
+      if constexpr (REFINE) {
+#pragma unroll
+        for (int k = 0; k < CB; ++k) b64[m][k] = 0.0;
+      }
+      if (r < n) {
+        const int vr = s.var[r], orr = s.obs[r];
+        double xr[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+          if (d < P.nlag) xr[d] = s.x[d][r];
+#pragma unroll
+        for (int k = 0; k < CB; ++k) {
+          if (k >= ncols) break;
+          double v;
+          if (k < pa) {
+            v = f_entry(P, k, vr, orr);
+          } else if (k < pa + q) {
+            const int iv = k - pa;
+            if (fast && !P.gstart) {
+              double lag[4];
+#pragma unroll
+              for (int d = 0; d < 4; ++d) {
+                const double dd = dsub(xr[d], d < P.nlag ? __ldg(&P.tx[d][t]) : 0.0);
+                lag[d] = (rs == 1.0) ? dd : dd / rs;
+              }
+              v = dadd(0.0, dmul(fast_cov(fm, zr, lag), 1.0));
+            } else {
+              v = rhs_cov_row(P, t, xr, vr, iv, rs);
+            }
+          } else {
+            const int u = k - pa - q;
+            v = u == 0 ? s.z[r] : (vr == u - 1 ? 1.0 : 0.0);
+          }
+          b[m][k] = (T)v;
+          if constexpr (REFINE) b64[m][k] = v;
+        }
+      }
+    }
+    // ---- K (assemble_lhs, lag = x_c - x_r): the n (n + 1) / 2 packed entries
+    // are spread evenly over the lanes and staged in shared memory, where
+    // the covariance calls do not hold the register matrix live
+    {
+      const int E = n * (n + 1) / 2;
+      int r = 0, c = lane;
+      while (c > r) { c -= r + 1; ++r; }
+      for (int e = lane; e < E; e += 32) {
+        const int vr = s.var[r];
+        double kv;
+        if (c == r) {
+          kv = dadd(dadd(cov0_pair(P, vr, vr), __ldg(&P.ovar[vr][s.obs[r]])), ln);
+        } else {
+          double lag[4];
+#pragma unroll
+          for (int d = 0; d < 4; ++d) {
+            const double dd = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
+            lag[d] = (P.st || rs == 1.0) ? dd : dd / rs;
+          }
+          kv = fast ? fast_cov(fm, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
+        }
+        s.K[e] = kv;
+        c += 32;
+        while (c > r) { c -= r + 1; ++r; }
+      }
+    }
+    __syncwarp();
+    T a[RI][CI];
+#pragma unroll
+    for (int ri = 0; ri < RI; ++ri) {
+      const int r = 4 * ri + pr;
+#pragma unroll
+      for (int ci = 0; ci < CI; ++ci) {
+        if (ri >= 2 * ci) {
+          const int c = 8 * ci + pc;
+          a[ri][ci] = (ri < nri && r < n && c <= r) ? (T)s.K[r * (r + 1) / 2 + c] : T(0);
+        }
+      }
+    }
+
+    if (P.ck_isa && lane == 0) {
+      for (int v = 0; v < q; ++v) {
+        const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
+        const int i1 = v + 1 >= q ? n : (v == 0 ? ist1 : (v == 1 ? ist2 : ist3));
+        double sz = 0.0;
+        for (int k = i0; k < i1; ++k) sz = dadd(sz, s.z[k]);
+        s.zmean[v] = i1 > i0 ? sz / (i1 - i0) : 0.0;
+        s.zmean[KK_MAXVAR + v] = (double)(i1 - i0);
+      }
+    }
+
+    // ---- right-looking Cholesky + forward substitution of b
+    bool fail = false;
+#pragma unroll
+    for (int jb = 0; jb < CI; ++jb) {
+      if (jb >= nci) break;
+      const int jm = (8 * jb) >> 5;  // right-hand-side slot of rows 8 jb .. 8 jb + 7
+#pragma unroll 1
+      for (int jj = 0; jj < 8; ++jj) {
+        const int j = 8 * jb + jj;
+        if (j >= n) break;
+        T* cw = s.col[j & 1];
+        const T dsel = (jj < 4) ? a[2 * jb][jb] : a[2 * jb + 1][jb];
+        const T d = __shfl_sync(FULL, dsel, jj * 4 + (jj & 3));
+        if (!(d > T(0))) { fail = true; break; }
+        const T inv = rsqrt_t(d);
+        if constexpr (REFINE) {
+          if (lane == 0) s.invd[j] = (float)inv;
+        }
+        if (pc == jj) {
+#pragma unroll
+          for (int ri = 2 * jb; ri < RI; ++ri) {
+            const int r = 4 * ri + pr;
+            const T l = (r > j) ? a[ri][jb] * inv : T(0);
+            if (REFINE) a[ri][jb] = l;
+            cw[pr * RI + ri] = l;
+          }
+        }
+        const int owner = ((j >> 2) & 7) * 4 + (j & 3);
+        if (lane == owner) {
+#pragma unroll
+          for (int k = 0; k < CB; ++k) {
+            if (k < ncols) {
+              const T yv = b[jm][k] * inv;
+              b[jm][k] = yv;
+              s.ybc[j & 1][k] = (double)yv;
+            }
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+          if (m < jm) continue;  // rows below 32 jm are finished
+          // L[r][j] for this lane's row r; the buffer holds column j only
+          // from row 8 jb on, and finished rows take no update
+          const T lb = (32 * m + 4 * pc + pr > j) ? cw[pr * RI + 8 * m + pc] : T(0);
+#pragma unroll
+          for (int k = 0; k < CB; ++k)
+            if (k < ncols) b[m][k] -= lb * (T)s.ybc[j & 1][k];
+        }
+        T lc[CI], lr[RI];
+#pragma unroll
+        for (int ci = jb; ci < CI; ++ci) lc[ci] = cw[(pc & 3) * RI + 2 * ci + (pc >> 2)];
+#pragma unroll
+        for (int ri = 2 * jb; ri < RI; ++ri) lr[ri] = cw[pr * RI + ri];
+#pragma unroll
+        for (int ci = jb; ci < CI; ++ci) {
+          if (ci >= nci) break;
+#pragma unroll
+          for (int ri = 2 * ci; ri < RI; ++ri) {
+            if (ri >= nri) break;
+            a[ri][ci] -= lr[ri] * lc[ci];
+          }
+        }
+      }
+      if (fail) break;
+    }
+    if (fail) {
+      // Cholesky failed: FP32 -> FP64 register kernel; FP64 -> generic LDL^T path
+      if (lane == 0) {
+        if (REFINE) {
+          P.status[t] |= KK_ST_FP64;
+          const int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
+          P.fp64_list[p] = t;
+        } else {
+          P.status[t] |= KK_ST_LDLT;
+          const int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
+          P.fb_list[p] = t;
+        }
+      }
+      __syncwarp();
+      continue;
+    }
+
+    if constexpr (!REFINE) {
+      // ---- G = Y^T Y over the forward-substituted columns
+#pragma unroll
+      for (int ka = 0; ka < MAXC; ++ka) {
+        if (ka >= C) break;
+#pragma unroll
+        for (int kb = ka; kb < MAXC; ++kb) {
+          if (kb >= C) break;
+          double g = 0.0;
+#pragma unroll
+          for (int m = 0; m < RM; ++m) g = fma((double)b[m][ka], (double)b[m][kb], g);
+          g = warp_sum(g);
+          if (lane == 0) {
+            s.G[ka * C + kb] = g;
+            s.G[kb * C + ka] = g;
+          }
+        }
+      }
+    } else {
+      // ---- keep L (FP32, strictly lower, packed by column) for the sweeps
+#pragma unroll
+      for (int ri = 0; ri < RI; ++ri) {
+        if (ri >= nri) break;
+        const int r = 4 * ri + pr;
+#pragma unroll
+        for (int ci = 0; ci < CI; ++ci) {
+          if (ri >= 2 * ci) {
+            const int c = 8 * ci + pc;
+            if (r > c && r < n) s.L[lcol<N>(c) + (r - c - 1)] = (float)a[ri][ci];
+          }
+        }
+      }
+      __syncwarp();
+      // backward sweep: x = L^-T y (y = the forward-substituted F | k)
+      auto back_sweep = [&](T (&v)[RM][CB]) {
+        for (int j = n - 1; j >= 0; --j) {
+          const int owner = ((j >> 2) & 7) * 4 + (j & 3);
+          const int jm2 = j >> 5;
+          const T ij = (T)s.invd[j];
+          T xj[CB];
+#pragma unroll
+          for (int k = 0; k < CB; ++k) {
+            if (k < nc) {
+              T mine = v[0][k];
+              if (RM > 1 && jm2 == 1) mine = v[RM - 1][k];
+              xj[k] = __shfl_sync(FULL, mine, owner) * ij;
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            const int r = 32 * m + 4 * pc + pr;
+            if (r == j) {
+#pragma unroll
+              for (int k = 0; k < CB; ++k)
+                if (k < nc) v[m][k] = xj[k];
+            } else if (r < j) {
+              const T l = (T)s.L[lcol<N>(r) + (j - r - 1)];
+#pragma unroll
+              for (int k = 0; k < CB; ++k)
+                if (k < nc) v[m][k] -= l * xj[k];
+            }
+          }
+        }
+      };
+      auto fwd_sweep = [&](T (&v)[RM][CB]) {
+        for (int j = 0; j < n; ++j) {
+          const int owner = ((j >> 2) & 7) * 4 + (j & 3);
+          const int jm2 = j >> 5;
+          const T ij = (T)s.invd[j];
+          T yj[CB];
+#pragma unroll
+          for (int k = 0; k < CB; ++k) {
+            if (k < nc) {
+              T mine = v[0][k];
+              if (RM > 1 && jm2 == 1) mine = v[RM - 1][k];
+              yj[k] = __shfl_sync(FULL, mine, owner) * ij;
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            const int r = 32 * m + 4 * pc + pr;
+            if (r == j) {
+#pragma unroll
+              for (int k = 0; k < CB; ++k)
+                if (k < nc) v[m][k] = yj[k];
+            } else if (r > j && r < n) {
+              const T l = (T)s.L[lcol<N>(j) + (r - j - 1)];
+#pragma unroll
+              for (int k = 0; k < CB; ++k)
+                if (k < nc) v[m][k] -= l * yj[k];
+            }
+          }
+        }
+      };
+      back_sweep(b);
+      double w[RM][CB];
+#pragma unroll
+      for (int m = 0; m < RM; ++m)
+#pragma unroll
+        for (int k = 0; k < CB; ++k) w[m][k] = (double)b[m][k];
+      // refinement: r = b64 - K64 w (FP64), dw = (L L^T)^-1 r (FP32)
+      bool conv = false;
+      double prev_rel = 0.0;
+      int it = 0;
+      for (; it < 3; ++it) {
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+          const int r = 32 * m + 4 * pc + pr;
+          if (r < n) {
+#pragma unroll
+            for (int k = 0; k < CB; ++k)
+              if (k < nc) s.W[k * N + r] = w[m][k];
+          }
+        }
+        __syncwarp();
+        T rr[RM][CB];
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+          const int r = 32 * m + 4 * pc + pr;
+          double acc[CB];
+#pragma unroll
+          for (int k = 0; k < CB; ++k) acc[k] = b64[m][k];
+          if (r < n) {
+            const int rowoff = r * (r + 1) / 2;
+            for (int c = 0; c < n; ++c) {
+              const double kv = c <= r ? s.K[rowoff + c] : s.K[c * (c + 1) / 2 + r];
+#pragma unroll
+              for (int k = 0; k < CB; ++k)
+                if (k < nc) acc[k] = fma(-kv, s.W[k * N + c], acc[k]);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < CB; ++k) rr[m][k] = (r < n && k < nc) ? (T)acc[k] : T(0);
+        }
+        fwd_sweep(rr);
+        back_sweep(rr);
+        double dmax = 0.0, wmax = 0.0;
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+          const int r = 32 * m + 4 * pc + pr;
+          if (r < n) {
+#pragma unroll
+            for (int k = 0; k < CB; ++k)
+              if (k < nc) {
+                w[m][k] += (double)rr[m][k];
+                dmax = fmax(dmax, fabs((double)rr[m][k]));
+                wmax = fmax(wmax, fabs(w[m][k]));
+              }
+          }
+        }
+        dmax = warp_max(dmax);
+        wmax = warp_max(wmax);
+        // error left after this step ~ rho * |dw| with rho the contraction of
+        // the FP32 solves, estimated from this and the previous step
+        const double rel = wmax > 0.0 ? dmax / wmax : 0.0;
+        const double rho = it == 0 ? rel : (prev_rel > 0.0 ? rel / prev_rel : 1.0);
+        prev_rel = rel;
+        __syncwarp();
+        if (10.0 * rho * rel <= P.refine_tol) { conv = true; ++it; break; }
+      }
+      n_iter += it;
+      if (!conv) {
+        if (lane == 0) {
+          P.status[t] |= KK_ST_FP64;
+          const int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
+          P.fp64_list[p] = t;
+        }
+        __syncwarp();
+        continue;
+      }
+      // ---- G[a][b] = col_a^T W_b for a in F | k | u, b in F | k
+#pragma unroll
+      for (int ka = 0; ka < MAXC; ++ka) {
+        if (ka >= C) break;
+#pragma unroll
+        for (int kb = 0; kb < CB; ++kb) {
+          if (kb >= nc) break;
+          double g = 0.0;
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            const int r = 32 * m + 4 * pc + pr;
+            if (r < n) {
+              double ca;
+              if (ka < nc) {
+                ca = b64[m][ka < CB ? ka : 0];
+              } else {
+                const int u = ka - nc;
+                ca = u == 0 ? s.z[r] : (s.var[r] == u - 1 ? 1.0 : 0.0);
+              }
+              g = fma(ca, w[m][kb], g);
+            }
+          }
+          g = warp_sum(g);
+          if (lane == 0) {
+            s.G[ka * C + kb] = g;
+            if (ka >= nc) s.G[kb * C + ka] = g;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      int f = 0;
+      finish_outputs(P, t, s.G, C, s.zmean, &f);
+      if (f) {
+        P.status[t] |= KK_ST_LDLT;
+        const int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
+        P.fb_list[p] = t;
+      } else {
+        ++n_chol;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (n_chol) atomicAdd(&P.counters[KK_CNT_CHOL], n_chol);
+    if (REFINE && n_iter) atomicAdd(&P.counters[KK_CNT_ITER], n_iter);
+  }
+}
+
+}  // namespace kk
