@@ -191,6 +191,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
+                    help="form of the timed leg (fp64 is for profiling the plain form alone)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -254,7 +256,7 @@ def main():
         return k
 
     # ---- FP32 + refinement (the measured form)
-    k32 = make("fp32_refine")
+    k32 = make(args.precision)
     sampler = ClockSampler(dev)
     tot32, times32 = time_steps(k32, args.steps, args.warmup, sampler)
     value = ntarget * world * args.steps / tot32
@@ -271,7 +273,7 @@ def main():
 
     # ---- FP64 plain
     fp64 = None
-    if not args.no_fp64:
+    if not args.no_fp64 and args.precision != "fp64":
         k64 = make("fp64")
         tot64, _ = time_steps(k64, args.steps, args.warmup)
         k64.profile(True)
@@ -359,11 +361,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot32 / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refinement",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 factor + f64 refinement" if args.precision == "fp32_refine" else "f64",
             "data": "synthetic (seeded, see bench_workloads.py)",
             "config": {"workload": w["name"], "ntargets": ntarget, "nobs": nobs,
                        "search": "anisotropic (0.5, az 30), 4 sectors x 16", "variogram": "exp r0.1 nug0.02",
-                       "precision": "fp32_refine", "l2": "flushed (256 MiB write) between timed steps",
+                       "precision": args.precision, "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"targets replicated per rank (weak), {world} GPU(s)"},
             "fp64_plain": fp64,
             "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,

@@ -481,7 +481,7 @@ void engine_solve(Engine& e) {
     e.stats[5] += nredo;
     if (nredo > 0) {
       if (!d.tree_ready) build_tree(e, v);
-      const int nthreads = std::min(nredo, 8192);
+      const int nthreads = std::min(nredo, 32768);
       const int stride = S.K + 2;
       DBuf heaps;
       heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);

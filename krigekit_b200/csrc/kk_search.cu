@@ -169,7 +169,68 @@ __device__ __forceinline__ long long sat_at(const KkGrid& g, int x, int y, int z
 }
 
 // count of points in the cell box [a, b] (inclusive, clipped)
-__device__ long long box_count(const KkGrid& g, const int* a, const int* b) {
+// Points in the grid cells that lie entirely inside the ball of squared
+// radius r2 around q (warp-wide sum; lanes take cell rows).  A lower bound
+// on the points within the ball, so the K-th nearest distance is at most
+// sqrt(r2) once it reaches K + 1.  Rounding is resolved towards counting
+// fewer cells.
+__device__ long long inner_count(const KkGrid& g, const double* q, double r2, int lane) {
+#pragma unroll
+  for (int d = 1; d < 4; ++d) {  // search dimensions without grid axis: their full extent
+    if (d >= g.G && d < g.D) {
+      const double e = fmax(fabs(q[d] - g.umin[d]), fabs(g.umax[d] - q[d]));
+      r2 -= e * e;
+    }
+  }
+  if (!(r2 > 0.0)) return 0;
+  r2 *= 1.0 - 1e-9;
+  double eps[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) eps[d] = 1e-12 * (fabs(g.lo[d]) + g.n[d] * g.h[d]);
+  const double r = sqrt(r2);
+  int cnt = 0;
+  if (g.G == 1) {
+    if (lane == 0) {
+      const int x0 = max(0, (int)ceil((q[0] - r + eps[0] - g.lo[0]) * g.inv_h[0]));
+      const int x1 = min(g.n[0] - 1, (int)floor((q[0] + r - eps[0] - g.lo[0]) * g.inv_h[0]) - 1);
+      if (x1 >= x0) cnt = __ldg(&g.cell_start[x1 + 1]) - __ldg(&g.cell_start[x0]);
+    }
+  } else {
+    const int y0 = max(0, (int)floor((q[1] - r - g.lo[1]) * g.inv_h[1]));
+    const int y1 = min(g.n[1] - 1, (int)floor((q[1] + r - g.lo[1]) * g.inv_h[1]));
+    int z0 = 0, z1 = 0;
+    if (g.G > 2) {
+      z0 = max(0, (int)floor((q[2] - r - g.lo[2]) * g.inv_h[2]));
+      z1 = min(g.n[2] - 1, (int)floor((q[2] + r - g.lo[2]) * g.inv_h[2]));
+    }
+    const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    if (ny > 0 && nz > 0) {
+      for (int p = lane; p < ny * nz; p += 32) {
+        const int y = y0 + p % ny, z = z0 + p / ny;
+        const double yl = g.lo[1] + y * g.h[1];
+        const double dy = fmax(fabs(q[1] - yl), fabs(yl + g.h[1] - q[1])) + eps[1];
+        double rem = r2 - dy * dy;
+        if (g.G > 2) {
+          const double zl = g.lo[2] + z * g.h[2];
+          const double dz = fmax(fabs(q[2] - zl), fabs(zl + g.h[2] - q[2])) + eps[2];
+          rem -= dz * dz;
+        }
+        if (rem <= 0.0) continue;
+        const double wx = sqrt(rem) - eps[0];
+        const int x0 = max(0, (int)ceil((q[0] - wx - g.lo[0]) * g.inv_h[0]));
+        const int x1 = min(g.n[0] - 1, (int)floor((q[0] + wx - g.lo[0]) * g.inv_h[0]) - 1);
+        if (x1 < x0) continue;
+        const int row = y * g.n[0] + z * g.n[0] * g.n[1];
+        cnt += __ldg(&g.cell_start[row + x1 + 1]) - __ldg(&g.cell_start[row + x0]);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  return cnt;
+}
+
+__device__ __forceinline__ long long box_count(const KkGrid& g, const int* a, const int* b) {
   int x0 = a[0], x1 = b[0] + 1;
   if (g.G == 1) return sat_at(g, x1, 0, 0) - sat_at(g, x0, 0, 0);
   int y0 = a[1], y1 = b[1] + 1;
@@ -184,9 +245,12 @@ __device__ long long box_count(const KkGrid& g, const int* a, const int* b) {
 // accumulation order sd = ((0 + d1^2) + d2^2) + ... (kdtree2_maxidx.f90:1547-1552)
 __device__ __forceinline__ double dist2(const KkGrid& g, const double* q, int j) {
   double sd = 0.0;
-  for (int d = 0; d < g.D; ++d) {
-    double t = dsub(__ldg(&g.sc[(size_t)d * g.nobs + j]), q[d]);
-    sd = dadd(sd, dmul(t, t));
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    if (d < g.D) {
+      double t = dsub(__ldg(&g.sc[(size_t)d * g.nobs + j]), q[d]);
+      sd = dadd(sd, dmul(t, t));
+    }
   }
   return sd;
 }
@@ -363,11 +427,22 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
   const double* os[4] = {o0, o1, o2, o3};
 
   for (int t = blockIdx.x * WARPS + w; t < ntarget; t += gridDim.x * WARPS) {
-    double x[4], q[4];
-    for (int d = 0; d < S.nlag; ++d) x[d] = __ldg(&ts[d][t]);
-    if (S.aniso) rotate_pt(S.rotmat, S.ndim, x, q);
-    else for (int d = 0; d < S.ndim; ++d) q[d] = x[d];
-    if (S.st) q[S.nlag - 1] = dmul(x[S.nlag - 1], S.ta);
+    double x[4] = {0.0, 0.0, 0.0, 0.0}, q[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+      if (d < S.nlag) x[d] = __ldg(&ts[d][t]);
+    if (S.aniso) {
+      rotate_pt(S.rotmat, S.ndim, x, q);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d < S.ndim) q[d] = x[d];
+    }
+    if (S.st) {
+#pragma unroll
+      for (int d = 1; d < 4; ++d)
+        if (d == S.nlag - 1) q[d] = dmul(x[d], S.ta);
+    }
     const int cvskip = S.cv ? t : -1;
     int st = 0;
     int nsel = 0;
@@ -379,13 +454,19 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
         int i = base + lane;
         bool keep = false;
         if (i < S.nobs && i != cvskip) {
-          double diff[3], r[3];
-          for (int d = 0; d < S.ndim; ++d) diff[d] = dsub(__ldg(&os[d][i]), S.st ? x[d] : q[d]);
+          double diff[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            if (d < S.ndim) diff[d] = dsub(__ldg(&os[d][i]), S.st ? x[d] : q[d]);
           rotate_pt(S.rotmat, S.ndim, diff, r);
           double s = 0.0;
-          for (int d = 0; d < S.ndim; ++d) s = dadd(s, dmul(r[d], r[d]));
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            if (d < S.ndim) s = dadd(s, dmul(r[d], r[d]));
           if (S.st) {
-            double tt = dsub(dmul(__ldg(&os[S.ndim][i]), S.ta), q[S.nlag - 1]);
+            const double* ot = S.ndim == 1 ? o1 : (S.ndim == 2 ? o2 : o3);
+            const double qt = S.nlag == 2 ? q[1] : (S.nlag == 3 ? q[2] : q[3]);
+            double tt = dsub(dmul(__ldg(&ot[i]), S.ta), qt);
             s = dadd(s, dmul(tt, tt));
           }
           keep = s <= S.maxd2;
@@ -400,21 +481,28 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
 
     // ---- grow the cell box until it holds K+1 points (or all points) ----
     const int K = S.K;  // K < nobs here
-    int c[3], a[3], bb[3];
-    for (int d = 0; d < g.G; ++d) c[d] = cell_coord(g, d, q[d]);
+    int c[4] = {0, 0, 0, 0}, a[4] = {0, 0, 0, 0}, bb[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (d < g.G) c[d] = cell_coord(g, d, q[d]);
     int R = 0;
     for (;; ++R) {
       bool full = true;
-      for (int d = 0; d < g.G; ++d) {
-        a[d] = max(0, c[d] - R);
-        bb[d] = min(g.n[d] - 1, c[d] + R);
-        if (a[d] > 0 || bb[d] < g.n[d] - 1) full = false;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (d < g.G) {
+          a[d] = max(0, c[d] - R);
+          bb[d] = min(g.n[d] - 1, c[d] + R);
+          if (a[d] > 0 || bb[d] < g.n[d] - 1) full = false;
+        }
       }
       if (full || box_count(g, a, bb) >= (long long)K + 1) break;
     }
     // farthest corner of the box (every search dimension), with a margin
     double D2 = 0.0;
-    for (int d = 0; d < g.D; ++d) {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (d >= g.D) break;
       double lo, hi;
       if (d < g.G) {
         lo = (a[d] == 0) ? fmin(g.umin[d], g.lo[d]) : g.lo[d] + a[d] * g.h[d];
@@ -425,6 +513,18 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
       }
       double e = fmax(fabs(q[d] - lo), fabs(hi - q[d]));
       D2 += e * e;
+    }
+    // tighten the radius: bisect for the smallest ball whose fully covered
+    // cells already hold K + 1 points (the corner ball of the box can reach
+    // far into a neighbouring cluster)
+    {
+      double rhi = sqrt(D2), rlo = 0.0;
+      for (int it = 0; it < 8; ++it) {
+        const double mid = 0.5 * (rlo + rhi);
+        if (inner_count(g, q, mid * mid, lane) >= (long long)K + 1) rhi = mid;
+        else rlo = mid;
+      }
+      D2 = fmin(D2, rhi * rhi);
     }
     D2 = D2 * (1.0 + 1e-9) + 1e-300;
     const double Dr = sqrt(D2);

@@ -37,7 +37,7 @@
 namespace kk {
 
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double rsqrt_t(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 
 // zone constants of the lookup tables, held in registers
 struct ZoneRegs {
@@ -96,8 +96,28 @@ __device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, in
   return cov_pair(P, first, second, lag);
 }
 
+// h = |M lag| with fused multiply-adds and h = h2 * rsqrt(h2): within a few
+// ulp of aniso_h, which moves the interpolated covariance by far less than
+// the solve tolerance (the table is continuous in h)
+__device__ __forceinline__ double aniso_h_fast(const double* m, int ndim, const double* lag) {
+  double h2;
+  if (ndim == 2) {
+    const double rx = fma(m[0], lag[0], m[3] * lag[1]);
+    const double ry = fma(m[1], lag[0], m[4] * lag[1]);
+    h2 = fma(rx, rx, ry * ry);
+  } else if (ndim == 3) {
+    const double rx = fma(m[0], lag[0], fma(m[3], lag[1], m[6] * lag[2]));
+    const double ry = fma(m[1], lag[0], fma(m[4], lag[1], m[7] * lag[2]));
+    const double rz = fma(m[2], lag[0], fma(m[5], lag[1], m[8] * lag[2]));
+    h2 = fma(rx, rx, fma(ry, ry, rz * rz));
+  } else {
+    return fabs(m[0] * lag[0]);
+  }
+  return h2 > 0.0 ? h2 * rsqrt(h2) : 0.0;
+}
+
 __device__ __forceinline__ double fast_cov(const FastModel& f, const ZoneRegs& z, const double* lag) {
-  const double h = aniso_h(f.m, f.ndim, lag);
+  const double h = aniso_h_fast(f.m, f.ndim, lag);
   if (h < z.zb3) return tab_fast(f.tab, z, h);
   return f.tail ? tail_cov(f.model, h) : 0.0;
 }
@@ -108,7 +128,7 @@ struct __align__(16) WarpSmem {
   double z[N];             // neighbour values
   int obs[N];
   int var[N];
-  T col[2][N];             // column j of L, layout [pr][ri]
+  T col[2][4 * (N / 4 + (sizeof(T) == 8 ? 2 : 4))];  // column j of L, layout [pr][ri], padded rows
   double ybc[2][MAXC];     // forward-substituted right-hand sides of row j
   double G[MAXC * MAXC];
   double zmean[2 * KK_MAXVAR];
@@ -151,6 +171,9 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   using WS = WarpSmem<T, N, REFINE>;
   constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
   constexpr int CB = REFINE ? KK_REFINE_COLS : MAXC;  // right-hand-side columns held per row
+  // column-buffer row stride: padded so the four row classes fall in
+  // different banks and stay 16-byte aligned
+  constexpr int RIP = RI + (sizeof(T) == 8 ? 2 : 4);
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WS& s = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
@@ -330,7 +353,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
             const int r = 4 * ri + pr;
             const T l = (r > j) ? a[ri][jb] * inv : T(0);
             if (REFINE) a[ri][jb] = l;
-            cw[pr * RI + ri] = l;
+            cw[pr * RIP + ri] = l;
           }
         }
         const int owner = ((j >> 2) & 7) * 4 + (j & 3);
@@ -350,22 +373,23 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
           if (m < jm) continue;  // rows below 32 jm are finished
           // L[r][j] for this lane's row r; the buffer holds column j only
           // from row 8 jb on, and finished rows take no update
-          const T lb = (32 * m + 4 * pc + pr > j) ? cw[pr * RI + 8 * m + pc] : T(0);
+          const T lb = (32 * m + 4 * pc + pr > j) ? cw[pr * RIP + 8 * m + pc] : T(0);
 #pragma unroll
           for (int k = 0; k < CB; ++k)
             if (k < ncols) b[m][k] -= lb * (T)s.ybc[j & 1][k];
         }
         T lc[CI], lr[RI];
 #pragma unroll
-        for (int ci = jb; ci < CI; ++ci) lc[ci] = cw[(pc & 3) * RI + 2 * ci + (pc >> 2)];
+        for (int ci = jb; ci < CI; ++ci) lc[ci] = cw[(pc & 3) * RIP + 2 * ci + (pc >> 2)];
 #pragma unroll
-        for (int ri = 2 * jb; ri < RI; ++ri) lr[ri] = cw[pr * RI + ri];
+        for (int ri = 2 * jb; ri < RI; ++ri) lr[ri] = cw[pr * RIP + ri];
+        // rows past n are zero: skip whole groups of four row slots
 #pragma unroll
         for (int ci = jb; ci < CI; ++ci) {
           if (ci >= nci) break;
 #pragma unroll
           for (int ri = 2 * ci; ri < RI; ++ri) {
-            if (ri >= nri) break;
+            if ((ri & 3) == 0 && ri >= nri) break;
             a[ri][ci] -= lr[ri] * lc[ci];
           }
         }
