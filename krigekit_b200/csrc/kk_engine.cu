@@ -350,6 +350,9 @@ static void fill_params(Engine& e, SolveParams& P) {
   P.fb_list = e.npp.as<int>();
   P.fp64_list = e.npp.as<int>() + nb;
   P.refine_tol = 1.0e-10;
+  // the refinement form's correction term c is about (cond * eps32)^2 of its
+  // value and carries an error of about c^1.5: c <= tol^(2/3) keeps it <= tol
+  P.refine_tol_corr = std::cbrt(P.refine_tol * P.refine_tol);
   if (P.pa + nv + 1 + ((P.ck_isa || P.sk_any) ? nv : 0) > 8)
     throw std::string("too many drift/variable columns for the register kernels (max 8)");
 }

@@ -48,6 +48,7 @@ struct SolveParams {
   double* scratch;           // generic-path workspace
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
+  double refine_tol_corr;    // bound on the FP32 correction term relative to its value
 };
 
 enum {

@@ -1048,7 +1048,8 @@ void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm
   const int* c = P.counters;
   const int* l32 = lists + (size_t)KK_CNT_B16 * P.nblock;
   const int* l64 = lists + (size_t)KK_CNT_B64 * P.nblock;
-  if (precision == 0 || P.pa + P.nvar > KK_REFINE_COLS) {
+  const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
+  if (precision == 0 || C > KK_REFINE_COLS) {
     launch_warp<double, 32, false>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
     launch_warp<double, 64, false>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
   } else {

@@ -30,9 +30,9 @@
 //      the same inner products are taken against the refined W.
 #pragma once
 
-// right-hand-side columns solved by the refinement form (F and k: pa + nvar);
-// systems with more columns are solved by the FP64 form
-#define KK_REFINE_COLS 4
+// right-hand-side columns carried by the refinement form (F | k | u); systems
+// with more columns are solved by the FP64 form
+#define KK_REFINE_COLS 6
 
 namespace kk {
 
@@ -183,8 +183,6 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   const int q = P.nvar, pa = P.pa;
   const int nu = n_func(P);
   const int C = pa + q + nu;  // forward-substituted columns (FP64 form)
-  const int nc = pa + q;      // solved columns (refinement form)
-  const int ncols = REFINE ? nc : C;
   const ZoneRegs zr = load_zones();
 
   FastModel fm;
@@ -252,7 +250,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
           if (d < P.nlag) xr[d] = s.x[d][r];
 #pragma unroll
         for (int k = 0; k < CB; ++k) {
-          if (k >= ncols) break;
+          if (k >= C) break;
           double v;
           if (k < pa) {
             v = f_entry(P, k, vr, orr);
@@ -360,7 +358,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         if (lane == owner) {
 #pragma unroll
           for (int k = 0; k < CB; ++k) {
-            if (k < ncols) {
+            if (k < C) {
               const T yv = b[jm][k] * inv;
               b[jm][k] = yv;
               s.ybc[j & 1][k] = (double)yv;
@@ -376,7 +374,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
           const T lb = (32 * m + 4 * pc + pr > j) ? cw[pr * RIP + 8 * m + pc] : T(0);
 #pragma unroll
           for (int k = 0; k < CB; ++k)
-            if (k < ncols) b[m][k] -= lb * (T)s.ybc[j & 1][k];
+            if (k < C) b[m][k] -= lb * (T)s.ybc[j & 1][k];
         }
         T lc[CI], lr[RI];
 #pragma unroll
@@ -446,18 +444,18 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         }
       }
       __syncwarp();
-      // backward sweep: x = L^-T y (y = the forward-substituted F | k)
-      auto back_sweep = [&](T (&v)[RM][CB]) {
+      // triangular sweeps over this lane's right-hand-side rows, L from
+      // shared memory, the pivot row's values broadcast by shuffle
+      auto back_sweep = [&](T (&v)[RM][CB]) {  // v <- L^-T v
         for (int j = n - 1; j >= 0; --j) {
           const int owner = ((j >> 2) & 7) * 4 + (j & 3);
-          const int jm2 = j >> 5;
           const T ij = (T)s.invd[j];
           T xj[CB];
 #pragma unroll
           for (int k = 0; k < CB; ++k) {
-            if (k < nc) {
+            if (k < C) {
               T mine = v[0][k];
-              if (RM > 1 && jm2 == 1) mine = v[RM - 1][k];
+              if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
               xj[k] = __shfl_sync(FULL, mine, owner) * ij;
             }
           }
@@ -467,27 +465,26 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
             if (r == j) {
 #pragma unroll
               for (int k = 0; k < CB; ++k)
-                if (k < nc) v[m][k] = xj[k];
+                if (k < C) v[m][k] = xj[k];
             } else if (r < j) {
               const T l = (T)s.L[lcol<N>(r) + (j - r - 1)];
 #pragma unroll
               for (int k = 0; k < CB; ++k)
-                if (k < nc) v[m][k] -= l * xj[k];
+                if (k < C) v[m][k] -= l * xj[k];
             }
           }
         }
       };
-      auto fwd_sweep = [&](T (&v)[RM][CB]) {
+      auto fwd_sweep = [&](T (&v)[RM][CB]) {  // v <- L^-1 v
         for (int j = 0; j < n; ++j) {
           const int owner = ((j >> 2) & 7) * 4 + (j & 3);
-          const int jm2 = j >> 5;
           const T ij = (T)s.invd[j];
           T yj[CB];
 #pragma unroll
           for (int k = 0; k < CB; ++k) {
-            if (k < nc) {
+            if (k < C) {
               T mine = v[0][k];
-              if (RM > 1 && jm2 == 1) mine = v[RM - 1][k];
+              if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
               yj[k] = __shfl_sync(FULL, mine, owner) * ij;
             }
           }
@@ -497,84 +494,82 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
             if (r == j) {
 #pragma unroll
               for (int k = 0; k < CB; ++k)
-                if (k < nc) v[m][k] = yj[k];
+                if (k < C) v[m][k] = yj[k];
             } else if (r > j && r < n) {
               const T l = (T)s.L[lcol<N>(j) + (r - j - 1)];
 #pragma unroll
               for (int k = 0; k < CB; ++k)
-                if (k < nc) v[m][k] -= l * yj[k];
+                if (k < C) v[m][k] -= l * yj[k];
             }
           }
         }
       };
+      // x = (L L^T)^-1 [F k u]: b holds L^-1 [F k u] from the factor sweep
       back_sweep(b);
-      double w[RM][CB];
 #pragma unroll
-      for (int m = 0; m < RM; ++m)
+      for (int m = 0; m < RM; ++m) {
+        const int r = 32 * m + 4 * pc + pr;
+        if (r < n) {
 #pragma unroll
-        for (int k = 0; k < CB; ++k) w[m][k] = (double)b[m][k];
-      // refinement: r = b64 - K64 w (FP64), dw = (L L^T)^-1 r (FP32)
-      bool conv = false;
-      double prev_rel = 0.0;
-      int it = 0;
-      for (; it < 3; ++it) {
-#pragma unroll
-        for (int m = 0; m < RM; ++m) {
-          const int r = 32 * m + 4 * pc + pr;
-          if (r < n) {
-#pragma unroll
-            for (int k = 0; k < CB; ++k)
-              if (k < nc) s.W[k * N + r] = w[m][k];
-          }
+          for (int k = 0; k < CB; ++k)
+            if (k < C) s.W[k * N + r] = (double)b[m][k];
         }
-        __syncwarp();
-        T rr[RM][CB];
-#pragma unroll
-        for (int m = 0; m < RM; ++m) {
-          const int r = 32 * m + 4 * pc + pr;
-          double acc[CB];
-#pragma unroll
-          for (int k = 0; k < CB; ++k) acc[k] = b64[m][k];
-          if (r < n) {
-            const int rowoff = r * (r + 1) / 2;
-            for (int c = 0; c < n; ++c) {
-              const double kv = c <= r ? s.K[rowoff + c] : s.K[c * (c + 1) / 2 + r];
-#pragma unroll
-              for (int k = 0; k < CB; ++k)
-                if (k < nc) acc[k] = fma(-kv, s.W[k * N + c], acc[k]);
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < CB; ++k) rr[m][k] = (r < n && k < nc) ? (T)acc[k] : T(0);
-        }
-        fwd_sweep(rr);
-        back_sweep(rr);
-        double dmax = 0.0, wmax = 0.0;
-#pragma unroll
-        for (int m = 0; m < RM; ++m) {
-          const int r = 32 * m + 4 * pc + pr;
-          if (r < n) {
-#pragma unroll
-            for (int k = 0; k < CB; ++k)
-              if (k < nc) {
-                w[m][k] += (double)rr[m][k];
-                dmax = fmax(dmax, fabs((double)rr[m][k]));
-                wmax = fmax(wmax, fabs(w[m][k]));
-              }
-          }
-        }
-        dmax = warp_max(dmax);
-        wmax = warp_max(wmax);
-        // error left after this step ~ rho * |dw| with rho the contraction of
-        // the FP32 solves, estimated from this and the previous step
-        const double rel = wmax > 0.0 ? dmax / wmax : 0.0;
-        const double rho = it == 0 ? rel : (prev_rel > 0.0 ? rel / prev_rel : 1.0);
-        prev_rel = rel;
-        __syncwarp();
-        if (10.0 * rho * rel <= P.refine_tol) { conv = true; ++it; break; }
       }
-      n_iter += it;
-      if (!conv) {
+      __syncwarp();
+      // K64 x (FP64) for this lane's rows, and the residuals r = col - K64 x
+      double kx[RM][CB];
+      T res[RM][CB];
+#pragma unroll
+      for (int m = 0; m < RM; ++m) {
+        const int r = 32 * m + 4 * pc + pr;
+#pragma unroll
+        for (int k = 0; k < CB; ++k) kx[m][k] = 0.0;
+        if (r < n) {
+          const int rowoff = r * (r + 1) / 2;
+          for (int c = 0; c < n; ++c) {
+            const double kv = c <= r ? s.K[rowoff + c] : s.K[c * (c + 1) / 2 + r];
+#pragma unroll
+            for (int k = 0; k < CB; ++k)
+              if (k < C) kx[m][k] = fma(kv, s.W[k * N + c], kx[m][k]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < CB; ++k) res[m][k] = (r < n && k < C) ? (T)(b64[m][k] - kx[m][k]) : T(0);
+      }
+      fwd_sweep(res);
+      // a^T K^-1 b = x_a^T b + x_b^T a - x_a^T K x_b + r_a^T K^-1 r_b exactly;
+      // the last term, taken with the FP32 factor, leaves an error of third
+      // order in the FP32 solution error
+      bool ok = true;
+#pragma unroll
+      for (int ka = 0; ka < CB; ++ka) {
+        if (ka >= C) break;
+#pragma unroll
+        for (int kb = ka; kb < CB; ++kb) {
+          if (kb >= C) break;
+          double g = 0.0, cr = 0.0;
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            const double xa = (double)b[m][ka], xb = (double)b[m][kb];
+            g = fma(xa, b64[m][kb], g);
+            g = fma(xb, b64[m][ka], g);
+            g = fma(-xa, kx[m][kb], g);
+            cr = fma((double)res[m][ka], (double)res[m][kb], cr);
+          }
+          g = warp_sum(g);
+          cr = warp_sum(cr);
+          g += cr;
+          // the correction is about (cond * eps32)^2 of the value and its own
+          // error one order higher: refine_tol_corr keeps that below refine_tol
+          if (ka == kb && !(cr <= P.refine_tol_corr * fabs(g))) ok = false;
+          if (lane == 0) {
+            s.G[ka * C + kb] = g;
+            s.G[kb * C + ka] = g;
+          }
+        }
+      }
+      ++n_iter;
+      if (!ok) {
         if (lane == 0) {
           P.status[t] |= KK_ST_FP64;
           const int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
@@ -582,35 +577,6 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         }
         __syncwarp();
         continue;
-      }
-      // ---- G[a][b] = col_a^T W_b for a in F | k | u, b in F | k
-#pragma unroll
-      for (int ka = 0; ka < MAXC; ++ka) {
-        if (ka >= C) break;
-#pragma unroll
-        for (int kb = 0; kb < CB; ++kb) {
-          if (kb >= nc) break;
-          double g = 0.0;
-#pragma unroll
-          for (int m = 0; m < RM; ++m) {
-            const int r = 32 * m + 4 * pc + pr;
-            if (r < n) {
-              double ca;
-              if (ka < nc) {
-                ca = b64[m][ka < CB ? ka : 0];
-              } else {
-                const int u = ka - nc;
-                ca = u == 0 ? s.z[r] : (s.var[r] == u - 1 ? 1.0 : 0.0);
-              }
-              g = fma(ca, w[m][kb], g);
-            }
-          }
-          g = warp_sum(g);
-          if (lane == 0) {
-            s.G[ka * C + kb] = g;
-            if (ka >= nc) s.G[kb * C + ka] = g;
-          }
-        }
       }
     }
     __syncwarp();
