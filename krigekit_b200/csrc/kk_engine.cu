@@ -502,6 +502,7 @@ void engine_solve(Engine& e) {
   // ---- solve parameters
   SolveParams P;
   fill_params(e, P);
+  P.fast_model = (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_B) ? 1 : 0;
 
   // ---- bucket + solve
   timer.start();

@@ -49,6 +49,7 @@ struct SolveParams {
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
   double refine_tol_corr;    // bound on the FP32 correction term relative to its value
+  int fast_model;            // one variable, spatial, one Level-B table: register fast path
 };
 
 enum {

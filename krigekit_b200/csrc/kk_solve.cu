@@ -1032,10 +1032,13 @@ static void launch_reg(const SolveParams& P, const int* list, const int* cnt, in
 template <typename T, int N, bool REFINE>
 static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
-  const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
+  // per-warp structs, then one packed K64 per warp
+  const size_t kbytes = sizeof(double) * (size_t)(N * (N + 1) / 2);
+  const size_t smem_max = (sizeof(WarpSmem<T, N, REFINE>) + kbytes) * WPC;
+  const size_t smem = smem_max;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
     attr_set = true;
   }
   int occ = 0;

@@ -132,7 +132,6 @@ struct __align__(16) WarpSmem {
   double ybc[2][MAXC];     // forward-substituted right-hand sides of row j
   double G[MAXC * MAXC];
   double zmean[2 * KK_MAXVAR];
-  double K[N * (N + 1) / 2];               // K64 packed row-major lower
   float L[REFINE ? N * (N - 1) / 2 : 1];   // FP32 factor, strictly lower, packed by column
   float invd[REFINE ? N : 1];              // 1 / L[j][j]
   double W[REFINE ? KK_REFINE_COLS * N : 1];         // current solution, broadcast for the residual
@@ -151,6 +150,62 @@ __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// Triangular sweeps of the refinement form over a lane's right-hand-side
+// rows r = 32 m + 4 pc + pr, with L (strictly lower, packed by column) and
+// 1 / L[j][j] in shared memory; the pivot row's values are broadcast by
+// shuffle from the lane that owns that row.
+template <typename T, int N, int RM, int CB>
+__device__ __forceinline__ void sweep_back(T (&v)[RM][CB], const float* __restrict__ L, const float* __restrict__ invd,
+                                           int n, int C, int lane) {  // v <- L^-T v
+  const int pr = lane & 3, pc = lane >> 2;
+  for (int j = n - 1; j >= 0; --j) {
+    const int owner = ((j >> 2) & 7) * 4 + (j & 3);
+    const T ij = (T)invd[j];
+    T xj[CB];
+#pragma unroll
+    for (int k = 0; k < CB; ++k) {
+      T mine = v[0][k];
+      if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
+      xj[k] = __shfl_sync(0xffffffffu, mine, owner) * ij;
+    }
+#pragma unroll
+    for (int m = 0; m < RM; ++m) {
+      const int r = 32 * m + 4 * pc + pr;
+      const T l = r < j ? (T)L[lcol<N>(r) + (j - r - 1)] : T(0);
+#pragma unroll
+      for (int k = 0; k < CB; ++k) {
+        if (k < C) v[m][k] = (r == j) ? xj[k] : v[m][k] - l * xj[k];
+      }
+    }
+  }
+}
+
+template <typename T, int N, int RM, int CB>
+__device__ __forceinline__ void sweep_fwd(T (&v)[RM][CB], const float* __restrict__ L, const float* __restrict__ invd,
+                                          int n, int C, int lane) {  // v <- L^-1 v
+  const int pr = lane & 3, pc = lane >> 2;
+  for (int j = 0; j < n; ++j) {
+    const int owner = ((j >> 2) & 7) * 4 + (j & 3);
+    const T ij = (T)invd[j];
+    T yj[CB];
+#pragma unroll
+    for (int k = 0; k < CB; ++k) {
+      T mine = v[0][k];
+      if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
+      yj[k] = __shfl_sync(0xffffffffu, mine, owner) * ij;
+    }
+#pragma unroll
+    for (int m = 0; m < RM; ++m) {
+      const int r = 32 * m + 4 * pc + pr;
+      const T l = (r > j && r < n) ? (T)L[lcol<N>(j) + (r - j - 1)] : T(0);
+#pragma unroll
+      for (int k = 0; k < CB; ++k) {
+        if (k < C) v[m][k] = (r == j) ? yj[k] : v[m][k] - l * yj[k];
+      }
+    }
+  }
 }
 
 // warps per CTA: the FP32 + refinement form at N = 64 keeps K64 and L in
@@ -177,6 +232,12 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WS& s = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+  // K64 packed row-major lower, after the per-warp structs: needed by the
+  // refinement residual and by models without the register fast path
+  constexpr int NK = N * (N + 1) / 2;
+  const bool fast = P.fast_model != 0;
+  double* Ks = reinterpret_cast<double*>(smem_raw + sizeof(WS) * warp_cta<T, N, REFINE>()) +
+               (size_t)(threadIdx.x >> 5) * NK;
   const int lane = threadIdx.x & 31;
   const int pr = lane & 3, pc = lane >> 2;
   const int n_items = *list_count;
@@ -186,7 +247,6 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   const ZoneRegs zr = load_zones();
 
   FastModel fm;
-  const bool fast = !P.st && q == 1 && P.models[0].mode == KK_LEVEL_B;
   if (fast) {
     const KkModel& m0 = P.models[0];
 #pragma unroll
@@ -218,6 +278,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
     }
     const double rs = P.rs ? __ldg(&P.rs[t]) : 1.0;
     const double ln = P.ln ? __ldg(&P.ln[t]) : 0.0;
+    const bool scale_lag = !P.st && rs != 1.0;  // warp-uniform
     for (int r = lane; r < n; r += 32) {
       const int v = (r >= ist1) + (r >= ist2) + (r >= ist3);
       const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
@@ -259,9 +320,10 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
             if (fast && !P.gstart) {
               double lag[4];
 #pragma unroll
-              for (int d = 0; d < 4; ++d) {
-                const double dd = dsub(xr[d], d < P.nlag ? __ldg(&P.tx[d][t]) : 0.0);
-                lag[d] = (rs == 1.0) ? dd : dd / rs;
+              for (int d = 0; d < 4; ++d) lag[d] = dsub(xr[d], d < P.nlag ? __ldg(&P.tx[d][t]) : 0.0);
+              if (scale_lag) {
+#pragma unroll
+                for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
               }
               v = dadd(0.0, dmul(fast_cov(fm, zr, lag), 1.0));
             } else {
@@ -276,9 +338,11 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         }
       }
     }
-    // ---- K (assemble_lhs, lag = x_c - x_r): the n (n + 1) / 2 packed entries
-    // are spread evenly over the lanes and staged in shared memory, where
-    // the covariance calls do not hold the register matrix live
+    // ---- K (assemble_lhs, lag = x_c - x_r)
+    T a[RI][CI];
+    // the packed entries are spread evenly over the lanes and staged in
+    // shared memory, where the covariance calls do not hold the register
+    // matrix live
     {
       const int E = n * (n + 1) / 2;
       int r = 0, c = lane;
@@ -291,19 +355,19 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         } else {
           double lag[4];
 #pragma unroll
-          for (int d = 0; d < 4; ++d) {
-            const double dd = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
-            lag[d] = (P.st || rs == 1.0) ? dd : dd / rs;
+          for (int d = 0; d < 4; ++d) lag[d] = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
+          if (scale_lag) {  // lag / rangescale (kriging.F90:783), only when a target sets it
+#pragma unroll
+            for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
           }
           kv = fast ? fast_cov(fm, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
         }
-        s.K[e] = kv;
+        Ks[e] = kv;
         c += 32;
         while (c > r) { c -= r + 1; ++r; }
       }
     }
     __syncwarp();
-    T a[RI][CI];
 #pragma unroll
     for (int ri = 0; ri < RI; ++ri) {
       const int r = 4 * ri + pr;
@@ -311,11 +375,10 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
       for (int ci = 0; ci < CI; ++ci) {
         if (ri >= 2 * ci) {
           const int c = 8 * ci + pc;
-          a[ri][ci] = (ri < nri && r < n && c <= r) ? (T)s.K[r * (r + 1) / 2 + c] : T(0);
+          a[ri][ci] = (ri < nri && r < n && c <= r) ? (T)Ks[r * (r + 1) / 2 + c] : T(0);
         }
       }
     }
-
     if (P.ck_isa && lane == 0) {
       for (int v = 0; v < q; ++v) {
         const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
@@ -444,68 +507,10 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         }
       }
       __syncwarp();
-      // triangular sweeps over this lane's right-hand-side rows, L from
-      // shared memory, the pivot row's values broadcast by shuffle
-      auto back_sweep = [&](T (&v)[RM][CB]) {  // v <- L^-T v
-        for (int j = n - 1; j >= 0; --j) {
-          const int owner = ((j >> 2) & 7) * 4 + (j & 3);
-          const T ij = (T)s.invd[j];
-          T xj[CB];
-#pragma unroll
-          for (int k = 0; k < CB; ++k) {
-            if (k < C) {
-              T mine = v[0][k];
-              if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
-              xj[k] = __shfl_sync(FULL, mine, owner) * ij;
-            }
-          }
-#pragma unroll
-          for (int m = 0; m < RM; ++m) {
-            const int r = 32 * m + 4 * pc + pr;
-            if (r == j) {
-#pragma unroll
-              for (int k = 0; k < CB; ++k)
-                if (k < C) v[m][k] = xj[k];
-            } else if (r < j) {
-              const T l = (T)s.L[lcol<N>(r) + (j - r - 1)];
-#pragma unroll
-              for (int k = 0; k < CB; ++k)
-                if (k < C) v[m][k] -= l * xj[k];
-            }
-          }
-        }
-      };
-      auto fwd_sweep = [&](T (&v)[RM][CB]) {  // v <- L^-1 v
-        for (int j = 0; j < n; ++j) {
-          const int owner = ((j >> 2) & 7) * 4 + (j & 3);
-          const T ij = (T)s.invd[j];
-          T yj[CB];
-#pragma unroll
-          for (int k = 0; k < CB; ++k) {
-            if (k < C) {
-              T mine = v[0][k];
-              if (RM > 1 && (j >> 5) == 1) mine = v[RM - 1][k];
-              yj[k] = __shfl_sync(FULL, mine, owner) * ij;
-            }
-          }
-#pragma unroll
-          for (int m = 0; m < RM; ++m) {
-            const int r = 32 * m + 4 * pc + pr;
-            if (r == j) {
-#pragma unroll
-              for (int k = 0; k < CB; ++k)
-                if (k < C) v[m][k] = yj[k];
-            } else if (r > j && r < n) {
-              const T l = (T)s.L[lcol<N>(j) + (r - j - 1)];
-#pragma unroll
-              for (int k = 0; k < CB; ++k)
-                if (k < C) v[m][k] -= l * yj[k];
-            }
-          }
-        }
-      };
+      const float* Lp = s.L;
+      const float* id = s.invd;
       // x = (L L^T)^-1 [F k u]: b holds L^-1 [F k u] from the factor sweep
-      back_sweep(b);
+      sweep_back<T, N, RM, CB>(b, Lp, id, n, C, lane);
 #pragma unroll
       for (int m = 0; m < RM; ++m) {
         const int r = 32 * m + 4 * pc + pr;
@@ -527,7 +532,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         if (r < n) {
           const int rowoff = r * (r + 1) / 2;
           for (int c = 0; c < n; ++c) {
-            const double kv = c <= r ? s.K[rowoff + c] : s.K[c * (c + 1) / 2 + r];
+            const double kv = c <= r ? Ks[rowoff + c] : Ks[c * (c + 1) / 2 + r];
 #pragma unroll
             for (int k = 0; k < CB; ++k)
               if (k < C) kx[m][k] = fma(kv, s.W[k * N + c], kx[m][k]);
@@ -536,7 +541,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
 #pragma unroll
         for (int k = 0; k < CB; ++k) res[m][k] = (r < n && k < C) ? (T)(b64[m][k] - kx[m][k]) : T(0);
       }
-      fwd_sweep(res);
+      sweep_fwd<T, N, RM, CB>(res, Lp, id, n, C, lane);
       // a^T K^-1 b = x_a^T b + x_b^T a - x_a^T K x_b + r_a^T K^-1 r_b exactly;
       // the last term, taken with the FP32 factor, leaves an error of third
       // order in the FP32 solution error
