@@ -152,6 +152,66 @@ def apply(k, w, set_grid=True):
     return k
 
 
+GQ4_FRAC = np.array([0.4305681558, 0.1699905218, -0.1699905218, -0.4305681558])  # gaussian_quadrature.f90
+GQ4_W = np.array([0.1739274226, 0.3260725774, 0.3260725774, 0.1739274226])
+
+
+def st_blocks(w, pad3d=False):
+    """Space-time targets of a config-5 workload as blocks: every block_every-th
+    target carries 4 x 4 Gauss-quadrature nodes over its grid cell at the
+    target time, the others one node at the target."""
+    g = w["grid"]
+    nd = g.shape[1] - 1
+    cell = w["cell"]
+    blk = (np.arange(len(g)) % w["block_every"]) == 0
+    nbp = np.where(blk, 16, 1).astype(np.int32)
+    ox, oy = np.meshgrid(GQ4_FRAC * cell, GQ4_FRAC * cell, indexing="ij")
+    wq = np.outer(GQ4_W, GQ4_W).ravel()
+    nodes, ntime, wts = [], [], []
+    for i in range(len(g)):
+        if blk[i]:
+            xy = np.column_stack([g[i, 0] + ox.ravel(), g[i, 1] + oy.ravel()])
+            nodes.append(xy)
+            ntime.append(np.full(16, g[i, nd]))
+            wts.append(wq)
+        else:
+            nodes.append(g[i:i + 1, :2])
+            ntime.append(g[i:i + 1, nd])
+            wts.append(np.ones(1))
+    nodes, ntime, wts = np.vstack(nodes), np.concatenate(ntime), np.concatenate(wts)
+    coord = g[:, :nd]
+    if pad3d:
+        coord = np.column_stack([coord, np.zeros(len(coord))])
+        nodes = np.column_stack([nodes, np.zeros(len(nodes))])
+    return dict(coord=coord, time=g[:, nd], nblockpnt=nbp, node_coord=nodes, node_time=ntime, weight=wts)
+
+
+def apply_st(k, w, blocks=True, pad3d=False):
+    """Configure a space-time kriging object (product or oracle) from a config-5 workload."""
+    m = w["st_model"]
+    k.set_st_model(model=m["model"], transform=m["transform"], at=m["at"], k_ps=m["k_ps"])
+    o = w["obs"][0]
+    c = o["coord"]
+    if pad3d:  # 2-D stations written as 3-D with z = 0, as the reference engine takes them
+        c = np.column_stack([c[:, :2], np.zeros(len(c)), c[:, 2]])
+    k.set_obs(1, c, o["value"], nmax=o.get("nmax"), maxdist=o.get("maxdist"))
+    for (i, j, spec) in w["vgm"]:
+        k.set_vgm(i, j, **spec)
+    for (i, j, spec) in w["vgm_t"]:
+        k.set_vgm_temporal(i, j, **spec)
+    b = st_blocks(w, pad3d)
+    if blocks:
+        if hasattr(k, "set_grid_nodes"):
+            k.set_grid_nodes(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
+        else:
+            k.set_grid_block(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
+    else:
+        k.set_grid(b["coord"], time=b["time"])
+    for iv, s in enumerate(w["search"], start=1):
+        k.set_search(iv, **s)
+    return k
+
+
 def rel_err(x, ref, floor):
     """|x - ref| / max(|ref|, floor), NaN-aware (NaN in both counts as equal)."""
     x = np.asarray(x, dtype=np.float64)

@@ -93,6 +93,52 @@ int krige_get_variance(int64_t handle, int nblocks, double *out);
 /* kriging_capi_common.F90:372-392 krige_get_variance_all: out(nblocks, nvar_c, nvar_c). */
 int krige_get_variance_all(int64_t handle, int nblocks, int nvar_c, double *out);
 
+/* ---- space-time kriging (kriging_st_capi.f90) ----
+ * Coordinates are the spatial ones followed by time.  krige_solve, the
+ * getters, krige_set_grid_cv, krige_update_obs_value and krige_set_obs_drift
+ * are shared with spatial kriging.  The reference engine is 3-D spatial + time;
+ * this library takes the spatial dimension (1..3) from the first
+ * krige_st_set_obs and expects spatial coordinate arrays of that dimension. */
+/* kriging_st_capi.f90:43-75 */
+int krige_st_create(int64_t *handle);
+int krige_st_destroy(int64_t *handle);
+/* kriging_st_capi.f90:80-123 krige_st_initialize -> t_kriging_st%initialize (std_ck cokriging). */
+int krige_st_initialize(int64_t handle, int nvar, int ndrift, int unbias, int nsim, int anisotropic_search,
+                        int weight_correction, int use_old_weight, int store_weight, int cross_validation,
+                        int write_mat, int neglect_error, int verbose, const char *weight_file,
+                        const double *bounds /* [2] */, int seed);
+/* kriging_st_capi.f90:128-162: model "sum_metric" | "product_sum", transform = variogram type of f(dt). */
+int krige_st_set_st_model(int64_t handle, const char *model, const char *transform, double at,
+                          double time_nugget, double time_sill, double k_ps);
+/* kriging_st_capi.f90:167-189: coord(ndim+1, nobs), last row = time. */
+int krige_st_set_obs(int64_t handle, int ivar, int nobs, int ndim, const double *coord, const double *value,
+                     const double *variance, int nmax, double maxdist, double sk_mean);
+/* kriging_st_capi.f90:245-258 */
+int krige_st_reset_vgm(int64_t handle, int ivar, int jvar);
+/* kriging_st_capi.f90:260-287: one spatial structure of vgm(ivar, jvar). */
+int krige_st_set_vgm(int64_t handle, int ivar, int jvar, const char *vtype, double nugget, double sill,
+                     double a_major, double a_minor1, double a_minor2, double azimuth, double dip,
+                     double plunge);
+/* kriging_st_capi.f90:289-309: one temporal structure (practical range at_k). */
+int krige_st_set_vgm_temporal(int64_t handle, int ivar, int jvar, const char *vtype, double nugget,
+                              double sill, double at_k);
+/* kriging_st_capi.f90:311-325: joint sills of the sum-metric model, one per spatial structure. */
+int krige_st_set_vgm_joint_sills(int64_t handle, int ivar, int jvar, int nsill, const double *sills);
+/* kriging_st_capi.f90:331-353: coord(ndim, ngrid), time(ngrid). */
+int krige_st_set_grid(int64_t handle, int ngrid, const double *coord, const double *time,
+                      const double *rangescale, const double *localnugget);
+/* kriging_st_capi.f90:355-388: block centres coord(ndim, nblocks) + time; integration nodes
+ * blockcoord(ndim, npnts_total) + blocktime with pointweight. */
+int krige_st_set_grid_block(int64_t handle, int nblocks, const double *coord, const double *time,
+                            const int *nblockpnt, int npnts_total, const double *blockcoord,
+                            const double *blocktime, const double *pointweight, const double *rangescale,
+                            const double *localnugget);
+/* kriging_st_capi.f90:392-406: drift(ndrift_c, nblocks), every variable. */
+int krige_st_set_grid_drift(int64_t handle, int ndrift_c, int nblocks, const double *drift);
+/* kriging_st_capi.f90:458-490 -> set_search (kriging_st.F90:322-403): search-space time = t * time_at. */
+int krige_st_set_search(int64_t handle, int ivar, double time_at, double anis1, double anis2, double azimuth,
+                        double dip, double plunge, int sector_search);
+
 /* ---- extensions of the GPU library (no counterpart in the reference) ---- */
 /* 0 = FP64 throughout, 1 = FP32 factorisation with FP64 iterative refinement (default). */
 int krige_set_precision(int64_t handle, int mode);

@@ -57,18 +57,21 @@ SIGNATURES = {
     "krige_get_variance_all": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
     # space-time entry points (kriging_st_capi.f90)
     "krige_st_create": ([_p_i64], _c_int),
-    "krige_st_initialize": ([_c_i64, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_double,
-                             _c_double, _c_int], _c_int),
-    "krige_st_set_st_model": ([_c_i64, _c_int, _c_int, _c_double, _c_double, _c_double, _c_double], _c_int),
+    "krige_st_destroy": ([_p_i64], _c_int),
+    "krige_st_initialize": ([_c_i64, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                             _c_int, _c_int, _c_int, _c_char_p, _p_dbl, _c_int], _c_int),
+    "krige_st_set_st_model": ([_c_i64, _c_char_p, _c_char_p, _c_double, _c_double, _c_double, _c_double], _c_int),
     "krige_st_set_obs": ([_c_i64, _c_int, _c_int, _c_int, _p_dbl, _p_dbl, _p_dbl, _c_int, _c_double, _c_double],
                          _c_int),
+    "krige_st_reset_vgm": ([_c_i64, _c_int, _c_int], _c_int),
     "krige_st_set_vgm": ([_c_i64, _c_int, _c_int, _c_char_p, _c_double, _c_double, _c_double, _c_double,
                           _c_double, _c_double, _c_double, _c_double], _c_int),
     "krige_st_set_vgm_temporal": ([_c_i64, _c_int, _c_int, _c_char_p, _c_double, _c_double, _c_double], _c_int),
     "krige_st_set_vgm_joint_sills": ([_c_i64, _c_int, _c_int, _c_int, _p_dbl], _c_int),
-    "krige_st_set_grid": ([_c_i64, _c_int, _c_int, _p_dbl, _p_dbl, _p_dbl, _p_dbl], _c_int),
-    "krige_st_set_grid_block": ([_c_i64, _c_int, _c_int, _p_dbl, _p_dbl, _p_int, _c_int, _p_dbl, _p_dbl, _p_dbl,
-                                 _p_dbl, _p_dbl], _c_int),
+    "krige_st_set_grid": ([_c_i64, _c_int, _p_dbl, _p_dbl, _p_dbl, _p_dbl], _c_int),
+    "krige_st_set_grid_block": ([_c_i64, _c_int, _p_dbl, _p_dbl, _p_int, _c_int, _p_dbl, _p_dbl, _p_dbl, _p_dbl,
+                                 _p_dbl], _c_int),
+    "krige_st_set_grid_drift": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
     "krige_st_set_search": ([_c_i64, _c_int, _c_double, _c_double, _c_double, _c_double, _c_double, _c_double,
                              _c_int], _c_int),
     # extensions of the GPU library

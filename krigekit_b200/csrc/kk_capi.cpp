@@ -70,6 +70,10 @@ using namespace kk;
 #define KK_GUARD_BEGIN \
   clear_error();       \
   try {
+#define KK_GUARD_END_NORET                     \
+  }                                            \
+  catch (const std::string& m) { set_error(m); } \
+  catch (const std::exception& x) { set_error(x.what()); }
 #define KK_GUARD_END                           \
   }                                            \
   catch (const std::string& m) { set_error(m); } \
@@ -627,6 +631,227 @@ int krige_gpu_phases(int64_t h, double* out4, int* launches) {
   for (int i = 0; i < 4; ++i) out4[i] = e->phase_ms[i];
   if (launches) *launches = e->launches;
   KK_GUARD_END
+}
+
+// ---------------------------------------------------------------------------
+// space-time kriging (kriging_st_capi.f90): coordinates are the spatial ones
+// followed by time; the shared entry points (krige_solve, the getters,
+// krige_set_grid_cv, krige_update_obs_value, krige_set_obs_drift) apply too
+// ---------------------------------------------------------------------------
+
+// krige_st_create / krige_st_destroy, kriging_st_capi.f90:43-75
+int krige_st_create(int64_t* handle) { return krige_create(handle); }
+int krige_st_destroy(int64_t* handle) { return krige_destroy(handle); }
+
+// krige_st_initialize, kriging_st_capi.f90:80-123 -> t_kriging_st%initialize
+// (the reference engine is 3-D spatial + time; here the spatial dimension is
+// taken from the first krige_st_set_obs, 3 until then)
+int krige_st_initialize(int64_t h, int nvar, int ndrift, int unbias, int nsim, int anisotropic_search,
+                        int weight_correction, int use_old_weight, int store_weight, int cross_validation,
+                        int write_mat, int neglect_error, int verbose, const char* weight_file,
+                        const double* bounds, int seed) {
+  if (krige_initialize(h, 3, nvar, ndrift, unbias, nsim, anisotropic_search, weight_correction, use_old_weight,
+                       store_weight, cross_validation, write_mat, neglect_error, 0, 1, verbose, 0, weight_file,
+                       bounds, seed) != 0)
+    return 1;
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  e->st = 1;
+  e->ndim = 3;
+  e->nlag = 4;
+  e->st_model = 0;
+  e->st_transform = KK_LIN;
+  e->st_at = 1.0;
+  e->st_k_ps = 0.0;
+  e->st_time_nugget = 0.0;
+  e->st_time_sill = 1.0;
+  KK_GUARD_END
+}
+
+static Engine* get_st(int64_t h) {
+  Engine* e = get(h);
+  if (e && !e->st) throw std::string("handle was not initialised by krige_st_initialize");
+  return e;
+}
+
+// krige_st_set_st_model, kriging_st_capi.f90:128-162
+int krige_st_set_st_model(int64_t h, const char* model, const char* transform, double at, double time_nugget,
+                          double time_sill, double k_ps) {
+  KK_GUARD_BEGIN
+  const std::string m = model ? model : "";
+  int imodel;
+  if (m == "sum_metric") imodel = 0;
+  else if (m == "product_sum") imodel = 1;
+  else throw std::string("model must be \"sum_metric\" or \"product_sum\", got: ") + m;
+  const int it = vtype_id(transform);
+  if (it < 0) throw std::string("Unknown variogram type: ") + (transform ? transform : "");
+  Engine* e = get_st(h);
+  if (!e) return 1;
+  e->st_model = imodel;
+  e->st_transform = it;
+  e->st_at = at;
+  e->st_time_nugget = time_nugget;
+  e->st_time_sill = time_sill;
+  e->st_k_ps = k_ps;
+  KK_GUARD_END
+}
+
+// krige_st_set_obs, kriging_st_capi.f90:167-189: coord(ndim+1, nobs)
+int krige_st_set_obs(int64_t h, int ivar, int nobs, int ndim, const double* coord, const double* value,
+                     const double* variance, int nmax, double maxdist, double sk_mean) {
+  {
+    KK_GUARD_BEGIN
+    Engine* e = get_st(h);
+    if (!e) return 1;
+    if (ndim < 1 || ndim > 3) throw std::string("ndim must be 1, 2 or 3");
+    bool any = false;
+    for (const ObsVar& o : e->obs) any = any || o.n > 0;
+    if (!any) {
+      e->ndim = ndim;
+      e->nlag = ndim + 1;
+    } else if (ndim != e->ndim) {
+      throw std::string("ndim differs from the observations already set");
+    }
+    KK_GUARD_END_NORET
+  }
+  if (failed()) return 1;
+  return krige_set_obs(h, ivar, nobs, ndim + 1, coord, value, variance, nmax, maxdist, sk_mean);
+}
+
+// krige_st_reset_vgm, kriging_st_capi.f90:245-258
+int krige_st_reset_vgm(int64_t h, int ivar, int jvar) {
+  KK_GUARD_BEGIN
+  Engine* e = get_st(h);
+  if (!e) return 1;
+  int a = std::min(ivar, jvar) - 1, b = std::max(ivar, jvar) - 1;
+  if (a < 0 || b >= e->nvar) throw std::string("ivar/jvar out of range");
+  e->vgm[a][b].clear();
+  e->vgm_t[a][b].clear();
+  e->joint[a][b].clear();
+  KK_GUARD_END
+}
+
+// krige_st_set_vgm, kriging_st_capi.f90:260-287: one spatial structure
+int krige_st_set_vgm(int64_t h, int ivar, int jvar, const char* vtype, double nugget, double sill, double a_major,
+                     double a_minor1, double a_minor2, double azimuth, double dip, double plunge) {
+  {
+    KK_GUARD_BEGIN
+    if (!get_st(h)) return 1;
+    KK_GUARD_END_NORET
+  }
+  if (failed()) return 1;
+  return krige_set_vgm(h, ivar, jvar, vtype, nugget, sill, a_major, a_minor1, a_minor2, azimuth, dip, plunge, 0);
+}
+
+// krige_st_set_vgm_temporal, kriging_st_capi.f90:289-309: one temporal structure
+int krige_st_set_vgm_temporal(int64_t h, int ivar, int jvar, const char* vtype, double nugget, double sill,
+                              double at_k) {
+  KK_GUARD_BEGIN
+  Engine* e = get_st(h);
+  if (!e) return 1;
+  if (ivar < 1 || jvar < 1 || ivar > e->nvar || jvar > e->nvar) throw std::string("ivar/jvar out of range");
+  const int id = vtype_id(vtype);
+  if (id < 0) throw std::string("Unknown variogram type: ") + (vtype ? vtype : "");
+  std::vector<StructSpec>& v = e->vgm_t[std::min(ivar, jvar) - 1][std::max(ivar, jvar) - 1];
+  if ((int)v.size() >= KK_MAXSTRUCT) throw std::string("exceeded the maximum number of nested structures");
+  StructSpec sp;
+  sp.vtype = id;
+  sp.nugget = nugget;
+  sp.sill = sill;
+  sp.a_major = at_k;
+  sp.a_minor1 = at_k;
+  sp.a_minor2 = at_k;
+  v.push_back(sp);
+  KK_GUARD_END
+}
+
+// krige_st_set_vgm_joint_sills, kriging_st_capi.f90:311-325: one sill per spatial structure
+int krige_st_set_vgm_joint_sills(int64_t h, int ivar, int jvar, int nsill, const double* sills) {
+  KK_GUARD_BEGIN
+  Engine* e = get_st(h);
+  if (!e) return 1;
+  if (ivar < 1 || jvar < 1 || ivar > e->nvar || jvar > e->nvar) throw std::string("ivar/jvar out of range");
+  const int a = std::min(ivar, jvar) - 1, b = std::max(ivar, jvar) - 1;
+  if (nsill != (int)e->vgm[a][b].size())
+    throw std::string("the number of joint sills must equal the number of spatial structures");
+  e->joint[a][b].assign(sills, sills + nsill);
+  KK_GUARD_END
+}
+
+// spatial coordinates (ndim, n) and times (n) -> (ndim + 1, n)
+static std::vector<double> st_coords(const Engine* e, int n, const double* coord, const double* time) {
+  const int nd = e->ndim;
+  std::vector<double> c((size_t)(nd + 1) * n);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < nd; ++k) c[(size_t)i * (nd + 1) + k] = coord[(size_t)i * nd + k];
+    c[(size_t)i * (nd + 1) + nd] = time[i];
+  }
+  return c;
+}
+
+// krige_st_set_grid, kriging_st_capi.f90:331-353: coord(ndim, ngrid), time(ngrid)
+int krige_st_set_grid(int64_t h, int ngrid, const double* coord, const double* time, const double* rangescale,
+                      const double* localnugget) {
+  std::vector<double> c;
+  {
+    KK_GUARD_BEGIN
+    Engine* e = get_st(h);
+    if (!e) return 1;
+    c = st_coords(e, ngrid, coord, time);
+    KK_GUARD_END_NORET
+  }
+  if (failed()) return 1;
+  int ndim = 0;
+  { Engine* e = get(h); ndim = e ? e->ndim : 0; }
+  return krige_set_grid(h, ngrid, ndim + 1, c.data(), rangescale, localnugget);
+}
+
+// krige_st_set_grid_block, kriging_st_capi.f90:355-388: block centres
+// coord(ndim, nblocks) + time, integration nodes blockcoord(ndim, npnts) +
+// blocktime with pointweight; the given centres are the search centres
+int krige_st_set_grid_block(int64_t h, int nblocks, const double* coord, const double* time, const int* nblockpnt,
+                            int npnts_total, const double* blockcoord, const double* blocktime,
+                            const double* pointweight, const double* rangescale, const double* localnugget) {
+  KK_GUARD_BEGIN
+  Engine* e = get_st(h);
+  if (!e) return 1;
+  if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
+  long long tot = 0;
+  for (int i = 0; i < nblocks; ++i) {
+    if (nblockpnt[i] <= 0) throw std::string("nblockpnt entries must be positive");
+    tot += nblockpnt[i];
+  }
+  if (tot != npnts_total) throw std::string("sum(nblockpnt) /= size(blockcoord, 2)");
+  e->bcoord = st_coords(e, nblocks, coord, time);
+  e->nblockpnt.assign(nblockpnt, nblockpnt + nblocks);
+  e->gcoord = st_coords(e, npnts_total, blockcoord, blocktime);
+  e->gweight.assign(pointweight, pointweight + npnts_total);
+  grid_common(e, nblocks, rangescale, localnugget);
+  KK_GUARD_END
+}
+
+// krige_st_set_grid_drift, kriging_st_capi.f90:392-406: drift(ndrift, nblocks), all variables
+int krige_st_set_grid_drift(int64_t h, int ndrift_c, int nblocks, const double* drift) {
+  return krige_set_grid_drift(h, -1, ndrift_c, nblocks, drift);
+}
+
+// krige_st_set_search, kriging_st_capi.f90:458-490 -> t_kriging_st%set_search
+// (kriging_st.F90:322-403): time_at scales the time axis of the search space
+int krige_st_set_search(int64_t h, int ivar, double time_at, double anis1, double anis2, double azimuth, double dip,
+                        double plunge, int sector_search) {
+  {
+    KK_GUARD_BEGIN
+    Engine* e = get_st(h);
+    if (!e) return 1;
+    if (!(time_at > 1.0e-10)) throw std::string("time_at must be positive.");
+    KK_GUARD_END_NORET
+  }
+  if (failed()) return 1;
+  if (krige_set_search(h, ivar, anis1, anis2, azimuth, dip, plunge, sector_search) != 0) return 1;
+  Engine* e = get(h);
+  e->obs[ivar - 1].time_at = time_at;
+  return 0;
 }
 
 // Allocation-free FP64 re-solve of the last krige_solve's neighbour sets

@@ -59,6 +59,9 @@ struct KkSTModel {
 struct KkGrid {
   int G;          // gridded dimensions (1..3)
   int D;          // search dimensions (nlag)
+  int gd[3];      // search dimension of each grid axis (the widest three when D = 4)
+  int gmask;      // bit d set when search dimension d is a grid axis
+  double gumin[3], gumax[3];  // bounding box of the grid axes
   int nobs;
   int n[3];       // cells per gridded dimension
   double lo[3], h[3], inv_h[3];

@@ -142,16 +142,35 @@ static void build_grid(Engine& e, int v) {
   }
   g.G = std::min(D, 3);
   g.nobs = n;
+  // grid axes: every search dimension, or with four (space-time in 3-D) the
+  // three of widest extent -- a constant coordinate (z = 0 for 2-D data
+  // given as 3-D) is then left out of the grid
+  int gd[3] = {0, 1, 2};
+  if (D > 3) {
+    int order[4] = {0, 1, 2, 3};
+    std::stable_sort(order, order + D, [&](int p, int q) {
+      return (g.umax[p] - g.umin[p]) > (g.umax[q] - g.umin[q]);
+    });
+    std::sort(order, order + 3);
+    for (int k = 0; k < 3; ++k) gd[k] = order[k];
+  }
+  g.gmask = 0;
+  for (int k = 0; k < 3; ++k) {
+    g.gd[k] = k < g.G ? gd[k] : 0;
+    if (k < g.G) g.gmask |= 1 << gd[k];
+    g.gumin[k] = k < g.G ? g.umin[gd[k]] : 0.0;
+    g.gumax[k] = k < g.G ? g.umax[gd[k]] : 0.0;
+  }
   // Cell size from the dense end of the point distribution: a coarse
   // histogram gives the density seen by the 99th-percentile point, and cells
   // are sized to hold about max(2, K/8) points there, so a K-nearest search
   // in the densest regions gathers a few K candidates while sparse regions
   // cost only extra (cheap, mostly empty) cell rows.
   double ext[3], vol = 1.0, emax = 0.0;
-  for (int k = 0; k < g.G; ++k) emax = std::max(emax, g.umax[k] - g.umin[k]);
+  for (int k = 0; k < g.G; ++k) emax = std::max(emax, g.gumax[k] - g.gumin[k]);
   if (emax <= 0.0) emax = 1.0;
   for (int k = 0; k < g.G; ++k) {
-    ext[k] = std::max(g.umax[k] - g.umin[k], 1e-9 * emax);
+    ext[k] = std::max(g.gumax[k] - g.gumin[k], 1e-9 * emax);
     vol *= ext[k];
   }
   const int nc_axis = g.G == 1 ? 65536 : (g.G == 2 ? 256 : 48);
@@ -161,7 +180,7 @@ static void build_grid(Engine& e, int v) {
   for (int i = 0; i < n; ++i) {
     long long c = 0, stride = 1;
     for (int k = 0; k < g.G; ++k) {
-      int ck = (int)((h[(size_t)k * n + i] - g.umin[k]) / ext[k] * nc_axis);
+      int ck = (int)((h[(size_t)gd[k] * n + i] - g.gumin[k]) / ext[k] * nc_axis);
       ck = ck < 0 ? 0 : (ck >= nc_axis ? nc_axis - 1 : ck);
       c += ck * stride;
       stride *= nc_axis;
@@ -195,7 +214,7 @@ static void build_grid(Engine& e, int v) {
   }
   for (int k = 0; k < 3; ++k) {
     if (k >= g.G) { g.n[k] = 1; g.lo[k] = 0; g.h[k] = 1; g.inv_h[k] = 1; continue; }
-    g.lo[k] = g.umin[k];
+    g.lo[k] = g.gumin[k];
     g.h[k] = ext[k] / g.n[k] * (1.0 + 1e-12);
     g.inv_h[k] = 1.0 / g.h[k];
   }

@@ -51,7 +51,7 @@ __global__ void k_cell_count(KkGrid g, const double* __restrict__ scu, int* __re
   if (i >= n) return;
   int c = 0, stride = 1;
   for (int d = 0; d < g.G; ++d) {
-    c += cell_coord(g, d, scu[(size_t)d * n + i]) * stride;
+    c += cell_coord(g, d, scu[(size_t)g.gd[d] * n + i]) * stride;
     stride *= g.n[d];
   }
   cell_of[i] = c;
@@ -174,11 +174,11 @@ __device__ __forceinline__ long long sat_at(const KkGrid& g, int x, int y, int z
 // on the points within the ball, so the K-th nearest distance is at most
 // sqrt(r2) once it reaches K + 1.  Rounding is resolved towards counting
 // fewer cells.
-__device__ long long inner_count(const KkGrid& g, const double* q, double r2, int lane) {
+__device__ long long inner_count(const KkGrid& g, const double* qa, const double* q, double r2, int lane) {
 #pragma unroll
-  for (int d = 1; d < 4; ++d) {  // search dimensions without grid axis: their full extent
-    if (d >= g.G && d < g.D) {
-      const double e = fmax(fabs(q[d] - g.umin[d]), fabs(g.umax[d] - q[d]));
+  for (int d = 0; d < 4; ++d) {  // search dimensions without grid axis: their full extent
+    if (d < g.D && !((g.gmask >> d) & 1)) {
+      const double e = fmax(fabs(qa[d] - g.umin[d]), fabs(g.umax[d] - qa[d]));
       r2 -= e * e;
     }
   }
@@ -482,9 +482,18 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
     // ---- grow the cell box until it holds K+1 points (or all points) ----
     const int K = S.K;  // K < nobs here
     int c[4] = {0, 0, 0, 0}, a[4] = {0, 0, 0, 0}, bb[4] = {0, 0, 0, 0};
+    // coordinates along the grid axes
+    double qg[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k < g.G) {
+        const int d = g.gd[k];
+        qg[k] = d == 0 ? q[0] : (d == 1 ? q[1] : (d == 2 ? q[2] : q[3]));
+      }
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      if (d < g.G) c[d] = cell_coord(g, d, q[d]);
+      if (d < g.G) c[d] = cell_coord(g, d, qg[d]);
     int R = 0;
     for (;; ++R) {
       bool full = true;
@@ -501,18 +510,20 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
     // farthest corner of the box (every search dimension), with a margin
     double D2 = 0.0;
 #pragma unroll
-    for (int d = 0; d < 4; ++d) {
-      if (d >= g.D) break;
-      double lo, hi;
-      if (d < g.G) {
-        lo = (a[d] == 0) ? fmin(g.umin[d], g.lo[d]) : g.lo[d] + a[d] * g.h[d];
-        hi = (bb[d] == g.n[d] - 1) ? fmax(g.umax[d], g.lo[d] + g.n[d] * g.h[d]) : g.lo[d] + (bb[d] + 1) * g.h[d];
-      } else {
-        lo = g.umin[d];
-        hi = g.umax[d];
-      }
-      double e = fmax(fabs(q[d] - lo), fabs(hi - q[d]));
+    for (int k = 0; k < 3; ++k) {
+      if (k >= g.G) break;
+      const double lo = (a[k] == 0) ? fmin(g.gumin[k], g.lo[k]) : g.lo[k] + a[k] * g.h[k];
+      const double hi = (bb[k] == g.n[k] - 1) ? fmax(g.gumax[k], g.lo[k] + g.n[k] * g.h[k])
+                                              : g.lo[k] + (bb[k] + 1) * g.h[k];
+      const double e = fmax(fabs(qg[k] - lo), fabs(hi - qg[k]));
       D2 += e * e;
+    }
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (d < g.D && !((g.gmask >> d) & 1)) {
+        const double e = fmax(fabs(q[d] - g.umin[d]), fabs(g.umax[d] - q[d]));
+        D2 += e * e;
+      }
     }
     // tighten the radius: bisect for the smallest ball whose fully covered
     // cells already hold K + 1 points (the corner ball of the box can reach
@@ -521,7 +532,7 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
       double rhi = sqrt(D2), rlo = 0.0;
       for (int it = 0; it < 8; ++it) {
         const double mid = 0.5 * (rlo + rhi);
-        if (inner_count(g, q, mid * mid, lane) >= (long long)K + 1) rhi = mid;
+        if (inner_count(g, q, qg, mid * mid, lane) >= (long long)K + 1) rhi = mid;
         else rlo = mid;
       }
       D2 = fmin(D2, rhi * rhi);
@@ -534,18 +545,18 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
     bool overflow = false;
     int zlo = 0, zhi = 0, ylo = 0, yhi = 0;
     if (g.G > 2) {
-      zlo = max(0, (int)floor((q[2] - Dr - g.lo[2]) * g.inv_h[2]) - 1);
-      zhi = min(g.n[2] - 1, (int)floor((q[2] + Dr - g.lo[2]) * g.inv_h[2]) + 1);
+      zlo = max(0, (int)floor((qg[2] - Dr - g.lo[2]) * g.inv_h[2]) - 1);
+      zhi = min(g.n[2] - 1, (int)floor((qg[2] + Dr - g.lo[2]) * g.inv_h[2]) + 1);
     }
     if (g.G > 1) {
-      ylo = max(0, (int)floor((q[1] - Dr - g.lo[1]) * g.inv_h[1]) - 1);
-      yhi = min(g.n[1] - 1, (int)floor((q[1] + Dr - g.lo[1]) * g.inv_h[1]) + 1);
+      ylo = max(0, (int)floor((qg[1] - Dr - g.lo[1]) * g.inv_h[1]) - 1);
+      yhi = min(g.n[1] - 1, (int)floor((qg[1] + Dr - g.lo[1]) * g.inv_h[1]) + 1);
     }
     for (int z = zlo; z <= zhi && !overflow; ++z) {
       double dz2 = 0.0;
       if (g.G > 2) {
         double zl = g.lo[2] + z * g.h[2] - 1e-6 * g.h[2], zh = zl + 1.000002 * g.h[2];
-        double dz = q[2] < zl ? zl - q[2] : (q[2] > zh ? q[2] - zh : 0.0);
+        double dz = qg[2] < zl ? zl - qg[2] : (qg[2] > zh ? qg[2] - zh : 0.0);
         dz2 = dz * dz;
         if (dz2 > D2) continue;
       }
@@ -553,13 +564,13 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
         double dy2 = dz2;
         if (g.G > 1) {
           double yl = g.lo[1] + y * g.h[1] - 1e-6 * g.h[1], yh = yl + 1.000002 * g.h[1];
-          double dy = q[1] < yl ? yl - q[1] : (q[1] > yh ? q[1] - yh : 0.0);
+          double dy = qg[1] < yl ? yl - qg[1] : (qg[1] > yh ? qg[1] - yh : 0.0);
           dy2 += dy * dy;
           if (dy2 > D2) continue;
         }
         double wx = sqrt(fmax(D2 - dy2, 0.0));
-        int x0 = max(0, (int)floor((q[0] - wx - g.lo[0]) * g.inv_h[0]) - 1);
-        int x1 = min(g.n[0] - 1, (int)floor((q[0] + wx - g.lo[0]) * g.inv_h[0]) + 1);
+        int x0 = max(0, (int)floor((qg[0] - wx - g.lo[0]) * g.inv_h[0]) - 1);
+        int x1 = min(g.n[0] - 1, (int)floor((qg[0] + wx - g.lo[0]) * g.inv_h[0]) + 1);
         int row = (g.G > 1 ? y : 0) * g.n[0] + (g.G > 2 ? z * g.n[0] * g.n[1] : 0);
         int p0 = __ldg(&g.cell_start[row + x0]);
         int p1 = __ldg(&g.cell_start[row + x1 + 1]);
