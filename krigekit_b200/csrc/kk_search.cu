@@ -394,9 +394,17 @@ __device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bc
   return true;
 }
 
+// Per-warp candidate buffers of k_search: CAP candidates {d2, idx, sector},
+// OCAP selected, BCAP boundary-bucket entries and the 256-bin histogram.
+// Sized so that three 4-warp CTAs fit on an SM; a target whose ball holds
+// more than CAP points, or that asks for OCAP or more candidates, takes the
+// exact kd-tree path instead.
+constexpr int KK_SEARCH_OCAP = 320;
+constexpr int KK_SEARCH_BCAP = 256;
 template <int CAP>
 __host__ __device__ constexpr size_t search_smem_per_warp() {
-  return sizeof(double) * (CAP + 512 + 256) + sizeof(int) * (CAP + 512 + 256 + 256) + CAP;
+  return sizeof(double) * (CAP + KK_SEARCH_OCAP + KK_SEARCH_BCAP) +
+         sizeof(int) * (CAP + KK_SEARCH_OCAP + KK_SEARCH_BCAP + 256) + CAP;
 }
 
 template <int CAP>
@@ -408,8 +416,8 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
                                                 int* __restrict__ nnear, int* __restrict__ status,
                                                 int* __restrict__ redo_list, int* __restrict__ redo_count) {
   constexpr int WARPS = 4;
-  constexpr int BCAP = 256;
-  constexpr int OCAP = 512;
+  constexpr int BCAP = KK_SEARCH_BCAP;
+  constexpr int OCAP = KK_SEARCH_OCAP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned char* base = smem_raw + (size_t)w * search_smem_per_warp<CAP>();
@@ -921,13 +929,13 @@ void launch_search(const KkSearch& S, int ntarget, const double* const* tx, cons
   int cap_blocks = nsm * 8;
   if (blocks > cap_blocks) blocks = cap_blocks;
   if (blocks < 1) blocks = 1;
-  const size_t smem = 4 * search_smem_per_warp<1024>();
+  const size_t smem = 4 * search_smem_per_warp<768>();
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_search<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_search<768>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  k_search<1024><<<blocks, 128, smem, st>>>(S, ntarget, tx[0], tx[1], tx[2], tx[3], ox[0], ox[1], ox[2], ox[3], nbr,
+  k_search<768><<<blocks, 128, smem, st>>>(S, ntarget, tx[0], tx[1], tx[2], tx[3], ox[0], ox[1], ox[2], ox[3], nbr,
                                         nnear, status, redo_list, redo_count);
 }
 
