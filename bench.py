@@ -33,6 +33,14 @@ import bench_workloads as bw  # noqa: E402
 
 METRIC = "kriged targets/s on 1 B200: FP32+refine batched vs FP64 plain at <=1e-6 rel err"
 
+# DRAM bytes per target of the dominant kernels, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload on its
+# 400 x 400 target grid (160 000 targets), scaled to a launch by the targets
+# it processes; the traffic is the neighbour lists and observation gathers and
+# grows in proportion to the targets.
+NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (52.349e6 + 0.751e6) / 160000,
+                             "search": (8.670e6 + 0.899e6) / 160000}
+
 
 def solve_flops(n, p=1, q=1):
     """Algorithmic FLOPs of one target system (Cholesky n^3/3, solves, Schur, variance)."""
@@ -379,12 +387,16 @@ def main():
             "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "accuracy": acc,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
-                         "frac": achieved / peaks["fp32"], "traffic": None,
-                         "kernel": "k_solve_reg<float,32|64,refine> (solve phase)",
+                         "frac": achieved / peaks["fp32"],
+                         "traffic": NCU_DRAM_BYTES_PER_TARGET["solve_fp32_refine"] * ntarget,
+                         "traffic_note": "ncu DRAM bytes per target (400x400 grid) x targets per launch",
+                         "kernel": "k_solve_warp<float,32|64,refine> (solve phase, CUDA-core FP32)",
                          "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live",
                          "flops_per_solve": flops, "solve_ms": ph32["solve_ms"]},
             "roofline_search": {"bound": "hbm", "achieved": search_gbs, "peak": hbm_gbs, "unit": "GB/s",
-                                "frac": search_gbs / hbm_gbs, "traffic": None, "peak_source": hbm_src,
+                                "frac": search_gbs / hbm_gbs,
+                                "traffic": NCU_DRAM_BYTES_PER_TARGET["search"] * ntarget,
+                                "kernel": "k_search<768>", "peak_source": hbm_src,
                                 "search_ms": ph32["search_ms"]},
             "peaks_measured_tflops": peaks,
             "phases_ms": ph32, "gpu_stats": gst,
