@@ -523,22 +523,47 @@ void engine_solve(Engine& e) {
   fill_params(e, P);
   P.fast_model = (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_B) ? 1 : 0;
 
-  // ---- bucket + solve
+  // ---- bucket by neighbour count
   timer.start();
   launch_bucket(P, e.bucket.as<int>(), st);
   timer.stop(1);
+  e.launches += 1;
+  int cb[KK_CNT_N];
+  KK_CUDA(cudaMemcpyAsync(cb, e.counters.p, sizeof cb, cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaStreamSynchronize(st));
+  // ---- solve: per chunk of a bucket list, the assembly kernel writes packed
+  // K64 to kbuf, then the factorisation kernel reads it
+  const int refine = solve_refine_form(P, e.precision);
+  constexpr int CH = 1 << 16;
+  const int nk64 = 64 * 65 / 2;
+  const int most = std::max(cb[KK_CNT_B16], cb[KK_CNT_B64]);
+  if (most > 0) e.kbuf.reserve(sizeof(double) * (size_t)std::min(CH, most) * nk64);
+  auto run_list = [&](const int* list, int count, int N, int form, int slot) {
+    for (int c0 = 0; c0 < count; c0 += CH) {
+      const int nit = std::min(CH, count - c0);
+      KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + slot, 0, sizeof(int), st));
+      launch_assemble(P, N, list, nullptr, c0, nit, e.kbuf.as<double>(), nsm, st);
+      launch_factor(P, form, N, list, nullptr, c0, nit, e.kbuf.as<double>(), slot, nsm, st);
+      KK_CUDA(cudaGetLastError());
+      e.launches += 2;
+    }
+  };
   timer.start();
-  launch_solve(P, e.precision, e.bucket.as<int>(), nsm, st);
-  KK_CUDA(cudaGetLastError());
+  run_list(e.bucket.as<int>() + (size_t)KK_CNT_B16 * nb, cb[KK_CNT_B16], 32, refine, KK_CNT_WORK0 + 0);
+  run_list(e.bucket.as<int>() + (size_t)KK_CNT_B64 * nb, cb[KK_CNT_B64], 64, refine, KK_CNT_WORK0 + 1);
   timer.stop(2);
-  e.launches += 3;
-  if (e.precision != 0) {
-    // FP32 targets whose refinement did not converge: FP64 register kernel
-    timer.start();
-    launch_solve_fp64_list(P, P.fp64_list, KK_CNT_FP64, nsm, st);
-    KK_CUDA(cudaGetLastError());
-    timer.stop(3);
-    e.launches += 1;
+  if (refine) {
+    // targets whose FP32 factorisation failed or whose correction check did
+    // not pass: FP64 form
+    int nf = 0;
+    KK_CUDA(cudaMemcpyAsync(&nf, e.counters.as<int>() + KK_CNT_FP64, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    if (nf > 0) {
+      e.kbuf.reserve(sizeof(double) * (size_t)std::min(CH, nf) * nk64);
+      timer.start();
+      run_list(P.fp64_list, nf, 64, 0, KK_CNT_WORK0 + 2);
+      timer.stop(3);
+    }
   }
   int cnt[KK_CNT_N];
   KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
@@ -644,7 +669,7 @@ void engine_release(Engine& e) {
   for (auto& b : e.gx) b.release();
   e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
   e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
-  e.counters.release(); e.scratch.release();
+  e.counters.release(); e.scratch.release(); e.kbuf.release();
 }
 
 }  // namespace kk

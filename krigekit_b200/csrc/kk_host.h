@@ -92,6 +92,7 @@ struct Engine {
   VarDevice vd[KK_MAXVAR];
   DBuf models, tables, tx[4], trs, tln, tdrift, gstart, gx[4], gw;
   DBuf est, var, status, npp, bucket, counters, scratch;
+  DBuf kbuf;  // packed K64 of one chunk of targets (assembly -> factorisation)
   size_t scratch_bytes = 0;
   int mmax_total = 0;
   bool solved = false;

@@ -78,8 +78,17 @@ void launch_search_kdtree(const KkSearch& S, const int* list, const int* count, 
 size_t kd_heap_entry_bytes();
 
 void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
-void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm, cudaStream_t st);
-void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_slot, int nsm, cudaStream_t st);
+// Warp-per-target solve of the targets list[item0 + i], i < nitems (or
+// < *cnt - item0 when cnt is given): k_assemble writes each target's packed
+// K64 to Kg + i * N (N + 1) / 2, then k_solve_warp factors and solves; N is
+// 32 or 64 (neighbour-count bucket); slot is the work counter, which must
+// start at zero.
+void launch_assemble(const SolveParams& P, int N, const int* list, const int* cnt, int item0, int nitems,
+                     double* Kg, int nsm, cudaStream_t st);
+void launch_factor(const SolveParams& P, int refine, int N, const int* list, const int* cnt, int item0, int nitems,
+                   const double* Kg, int slot, int nsm, cudaStream_t st);
+// 1 when the FP32 + refinement form applies (precision 1 and few enough columns)
+int solve_refine_form(const SolveParams& P, int precision);
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st);
 void set_zones(cudaStream_t st);
 

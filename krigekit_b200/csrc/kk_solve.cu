@@ -1030,41 +1030,47 @@ static void launch_reg(const SolveParams& P, const int* list, const int* cnt, in
 }
 
 template <typename T, int N, bool REFINE>
-static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int slot, int nsm, cudaStream_t st) {
+static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
+                        const double* Kg, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
-  // per-warp structs, then one packed K64 per warp
-  const size_t kbytes = sizeof(double) * (size_t)(N * (N + 1) / 2);
-  const size_t smem_max = (sizeof(WarpSmem<T, N, REFINE>) + kbytes) * WPC;
-  const size_t smem = smem_max;
+  const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_set = true;
   }
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE>, 32 * WPC, smem);
   if (occ < 1) occ = 1;
-  k_solve_warp<T, N, REFINE><<<nsm * occ, 32 * WPC, smem, st>>>(P, list, cnt, slot);
+  int blocks = nsm * occ;
+  const int need = (nitems + WPC - 1) / WPC;
+  if (need < blocks) blocks = need > 0 ? need : 1;
+  k_solve_warp<T, N, REFINE><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
 }
 
-void launch_solve(const SolveParams& P, int precision, const int* lists, int nsm, cudaStream_t st) {
-  const int* c = P.counters;
-  const int* l32 = lists + (size_t)KK_CNT_B16 * P.nblock;
-  const int* l64 = lists + (size_t)KK_CNT_B64 * P.nblock;
+int solve_refine_form(const SolveParams& P, int precision) {
   const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
-  if (precision == 0 || C > KK_REFINE_COLS) {
-    launch_warp<double, 32, false>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
-    launch_warp<double, 64, false>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
-  } else {
-    launch_warp<float, 32, true>(P, l32, c + KK_CNT_B16, KK_CNT_WORK0 + 0, nsm, st);
-    launch_warp<float, 64, true>(P, l64, c + KK_CNT_B64, KK_CNT_WORK0 + 1, nsm, st);
-  }
+  return precision != 0 && C <= KK_REFINE_COLS;
 }
 
-// FP64 solve of an explicit list of targets with at most 64 neighbours (FP32
-// refinement that did not converge, or an FP32 factorisation that failed)
-void launch_solve_fp64_list(const SolveParams& P, const int* list, int list_cnt_slot, int nsm, cudaStream_t st) {
-  launch_warp<double, 64, false>(P, list, P.counters + list_cnt_slot, KK_CNT_WORK0 + 2, nsm, st);
+void launch_assemble(const SolveParams& P, int N, const int* list, const int* cnt, int item0, int nitems,
+                     double* Kg, int nsm, cudaStream_t st) {
+  int blocks = nsm * 4;
+  const int need = (nitems + 7) / 8;
+  if (need < blocks) blocks = need > 0 ? need : 1;
+  if (N == 32) k_assemble<32><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+  else k_assemble<64><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+}
+
+void launch_factor(const SolveParams& P, int refine, int N, const int* list, const int* cnt, int item0, int nitems,
+                   const double* Kg, int slot, int nsm, cudaStream_t st) {
+  if (refine) {
+    if (N == 32) launch_warp<float, 32, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    else launch_warp<float, 64, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+  } else {
+    if (N == 32) launch_warp<double, 32, false>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    else launch_warp<double, 64, false>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+  }
 }
 
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st) {

@@ -208,10 +208,112 @@ __device__ __forceinline__ void sweep_fwd(T (&v)[RM][CB], const float* __restric
   }
 }
 
-// warps per CTA: the FP32 + refinement form at N = 64 keeps K64 and L in
-// shared memory (about 33 KB per warp), so it runs two warps per CTA
+// Neighbour rows of target t in matrix order (variable blocks in order,
+// ascending index within a block: assemble_linear_system_base,
+// kriging_base.F90:3159-3235) into per-warp shared arrays.  Returns the row
+// count n and the block starts of variables 1..3.
+template <int N>
+__device__ __forceinline__ int gather_rows(const SolveParams& P, int t, int lane, double (*x)[N], double* z,
+                                           int* obs, int* var, int& ist1, int& ist2, int& ist3) {
+  const int q = P.nvar;
+  int n = 0;
+  ist1 = ist2 = ist3 = 0x7fffffff;
+#pragma unroll
+  for (int v = 0; v < KK_MAXVAR; ++v) {
+    if (v < q) {
+      if (v == 1) ist1 = n;
+      if (v == 2) ist2 = n;
+      if (v == 3) ist3 = n;
+      n += __ldg(&P.nnear[v][t]);
+    }
+  }
+  for (int r = lane; r < n; r += 32) {
+    const int v = (r >= ist1) + (r >= ist2) + (r >= ist3);
+    const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
+    const int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (r - i0)]);
+    obs[r] = o;
+    var[r] = v;
+    for (int d = 0; d < P.nlag; ++d) x[d][r] = __ldg(&P.ox[v][d][o]);
+    if (z) z[r] = __ldg(&P.oval[v][o]);
+  }
+  __syncwarp();
+  return n;
+}
+
+// Covariance matrix K (assemble_lhs, kriging.F90:714-849; lag = x_c - x_r,
+// diagonal cov0 + observation variance + local nugget) of the targets
+// list[item0 + i], i < count, written packed row-major lower to
+// Kg + i * N (N + 1) / 2.  One warp per target; the packed entries are
+// spread evenly over the lanes (stores are contiguous across the warp).
+// This is the part of the solve that is bound by covariance-table latency,
+// so it runs as its own kernel with many resident warps; the factorisation
+// kernel then reads K from this buffer (L2-resident in chunks).
+template <int N>
+__global__ void __launch_bounds__(256, 4) k_assemble(const __grid_constant__ SolveParams P,
+                                                     const int* __restrict__ list,
+                                                     const int* __restrict__ list_count, int item0, int nitems,
+                                                     double* __restrict__ Kg) {
+  constexpr int NK = N * (N + 1) / 2;
+  struct Rows {
+    double x[4][N];
+    int obs[N];
+    int var[N];
+  };
+  __shared__ Rows rows[8];
+  Rows& s = rows[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  int count = nitems;
+  if (list_count) count = min(nitems, *list_count - item0);
+  const bool fast = P.fast_model != 0;
+  const ZoneRegs zr = load_zones();
+  FastModel fm;
+  if (fast) {
+    const KkModel& m0 = P.models[0];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fm.m[k] = m0.bmat[k];
+    fm.tab = P.tables + m0.btab_off;
+    fm.model = &m0;
+    fm.ndim = m0.ndim;
+    fm.tail = m0.btail;
+  }
+  const int nwarp = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < count; it += nwarp) {
+    const int t = __ldg(&list[item0 + it]);
+    int ist1, ist2, ist3;
+    const int n = gather_rows<N>(P, t, lane, s.x, nullptr, s.obs, s.var, ist1, ist2, ist3);
+    const double rs = P.rs ? __ldg(&P.rs[t]) : 1.0;
+    const double ln = P.ln ? __ldg(&P.ln[t]) : 0.0;
+    const bool scale_lag = !P.st && rs != 1.0;  // warp-uniform
+    double* K = Kg + (size_t)it * NK;
+    const int E = n * (n + 1) / 2;
+    int r = 0, c = lane;
+    while (c > r) { c -= r + 1; ++r; }
+    for (int e = lane; e < E; e += 32) {
+      const int vr = s.var[r];
+      double kv;
+      if (c == r) {
+        kv = dadd(dadd(cov0_pair(P, vr, vr), __ldg(&P.ovar[vr][s.obs[r]])), ln);
+      } else {
+        double lag[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) lag[d] = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
+        if (scale_lag) {  // lag / rangescale (kriging.F90:783), only when a target sets it
+#pragma unroll
+          for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
+        }
+        kv = fast ? fast_cov(fm, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
+      }
+      K[e] = kv;
+      c += 32;
+      while (c > r) { c -= r + 1; ++r; }
+    }
+    __syncwarp();
+  }
+}
+
+// warps per CTA of the factorisation kernel
 template <typename T, int N, bool REFINE>
-constexpr int warp_cta() { return (REFINE && N == 64) ? 2 : 4; }
+constexpr int warp_cta() { return 4; }
 
 // CTAs per SM the register budget is sized for (the launch bound caps the
 // registers at 64 K / (threads * this)): the N = 64 forms need the whole
@@ -222,7 +324,8 @@ constexpr int warp_min_ctas() { return N == 64 ? 1 : 4; }
 template <typename T, int N, bool REFINE>
 __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE>())
     k_solve_warp(const __grid_constant__ SolveParams P, const int* __restrict__ list,
-                 const int* __restrict__ list_count, int work_slot) {
+                 const int* __restrict__ list_count, int item0, int nitems, const double* __restrict__ Kg,
+                 int work_slot) {
   using WS = WarpSmem<T, N, REFINE>;
   constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
   constexpr int CB = REFINE ? KK_REFINE_COLS : MAXC;  // right-hand-side columns held per row
@@ -232,15 +335,12 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WS& s = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
-  // K64 packed row-major lower, after the per-warp structs: needed by the
-  // refinement residual and by models without the register fast path
-  constexpr int NK = N * (N + 1) / 2;
+  constexpr int NK = N * (N + 1) / 2;  // packed K64 of one target in Kg (from k_assemble)
   const bool fast = P.fast_model != 0;
-  double* Ks = reinterpret_cast<double*>(smem_raw + sizeof(WS) * warp_cta<T, N, REFINE>()) +
-               (size_t)(threadIdx.x >> 5) * NK;
   const int lane = threadIdx.x & 31;
   const int pr = lane & 3, pc = lane >> 2;
-  const int n_items = *list_count;
+  int n_items = nitems;
+  if (list_count) n_items = min(nitems, *list_count - item0);
   const int q = P.nvar, pa = P.pa;
   const int nu = n_func(P);
   const int C = pa + q + nu;  // forward-substituted columns (FP64 form)
@@ -263,32 +363,14 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
     if (lane == 0) item = atomicAdd(&P.counters[work_slot], 1);
     item = __shfl_sync(FULL, item, 0);
     if (item >= n_items) break;
-    const int t = __ldg(&list[item]);
+    const int t = __ldg(&list[item0 + item]);
+    const double* Ks = Kg + (size_t)item * NK;
 
     // ---- neighbour rows: variable blocks in order, ascending index
-    int ist1 = 0x7fffffff, ist2 = 0x7fffffff, ist3 = 0x7fffffff, n = 0;
-#pragma unroll
-    for (int v = 0; v < KK_MAXVAR; ++v) {
-      if (v < q) {
-        if (v == 1) ist1 = n;
-        if (v == 2) ist2 = n;
-        if (v == 3) ist3 = n;
-        n += __ldg(&P.nnear[v][t]);
-      }
-    }
+    int ist1, ist2, ist3;
+    const int n = gather_rows<N>(P, t, lane, s.x, s.z, s.obs, s.var, ist1, ist2, ist3);
     const double rs = P.rs ? __ldg(&P.rs[t]) : 1.0;
-    const double ln = P.ln ? __ldg(&P.ln[t]) : 0.0;
     const bool scale_lag = !P.st && rs != 1.0;  // warp-uniform
-    for (int r = lane; r < n; r += 32) {
-      const int v = (r >= ist1) + (r >= ist2) + (r >= ist3);
-      const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
-      const int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (r - i0)]);
-      s.obs[r] = o;
-      s.var[r] = v;
-      for (int d = 0; d < P.nlag; ++d) s.x[d][r] = __ldg(&P.ox[v][d][o]);
-      s.z[r] = __ldg(&P.oval[v][o]);
-    }
-    __syncwarp();
     const int nri = (n + 3) >> 2, nci = (n + 7) >> 3;
 
     // ---- right-hand-side rows r = 32 m + 4 pc + pr: F (pa), k (q), u (nu)
@@ -338,36 +420,8 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         }
       }
     }
-    // ---- K (assemble_lhs, lag = x_c - x_r)
+    // ---- K from the assembly kernel (packed row-major lower, FP64)
     T a[RI][CI];
-    // the packed entries are spread evenly over the lanes and staged in
-    // shared memory, where the covariance calls do not hold the register
-    // matrix live
-    {
-      const int E = n * (n + 1) / 2;
-      int r = 0, c = lane;
-      while (c > r) { c -= r + 1; ++r; }
-      for (int e = lane; e < E; e += 32) {
-        const int vr = s.var[r];
-        double kv;
-        if (c == r) {
-          kv = dadd(dadd(cov0_pair(P, vr, vr), __ldg(&P.ovar[vr][s.obs[r]])), ln);
-        } else {
-          double lag[4];
-#pragma unroll
-          for (int d = 0; d < 4; ++d) lag[d] = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
-          if (scale_lag) {  // lag / rangescale (kriging.F90:783), only when a target sets it
-#pragma unroll
-            for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
-          }
-          kv = fast ? fast_cov(fm, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
-        }
-        Ks[e] = kv;
-        c += 32;
-        while (c > r) { c -= r + 1; ++r; }
-      }
-    }
-    __syncwarp();
 #pragma unroll
     for (int ri = 0; ri < RI; ++ri) {
       const int r = 4 * ri + pr;
@@ -375,7 +429,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
       for (int ci = 0; ci < CI; ++ci) {
         if (ri >= 2 * ci) {
           const int c = 8 * ci + pc;
-          a[ri][ci] = (ri < nri && r < n && c <= r) ? (T)Ks[r * (r + 1) / 2 + c] : T(0);
+          a[ri][ci] = (ri < nri && r < n && c <= r) ? (T)__ldg(&Ks[r * (r + 1) / 2 + c]) : T(0);
         }
       }
     }
@@ -532,7 +586,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         if (r < n) {
           const int rowoff = r * (r + 1) / 2;
           for (int c = 0; c < n; ++c) {
-            const double kv = c <= r ? Ks[rowoff + c] : Ks[c * (c + 1) / 2 + r];
+            const double kv = c <= r ? __ldg(&Ks[rowoff + c]) : __ldg(&Ks[c * (c + 1) / 2 + r]);
 #pragma unroll
             for (int k = 0; k < CB; ++k)
               if (k < C) kx[m][k] = fma(kv, s.W[k * N + c], kx[m][k]);
