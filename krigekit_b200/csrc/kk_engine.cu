@@ -103,6 +103,8 @@ static void setup_search(Engine& e, int v, KkSearch& S) {
     S.K = o.n;
     S.mmax = o.n;
   } else if (o.sector) {
+    // the sector selection packs the sector id above bit 28 of the index
+    if (o.n >= (1 << 28)) throw std::string("sector search supports fewer than 2^28 observations per variable");
     S.mode = 2;
     long long lim = (long long)(1 << e.ndim) * nmax * 4;
     S.K = (int)std::min<long long>(o.n, lim);

@@ -394,6 +394,146 @@ __device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bc
   return true;
 }
 
+// Bitonic sort of (key, idx) pairs in shared memory by (idx >> 28, key,
+// idx): the sector id rides in bits 28..30 of idx (observation indices are
+// below 2^28 in sector mode).
+__device__ void warp_sort_sec(double* key, int* idx, int n) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= n; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < n; i += 32) {
+        int p = i ^ j;
+        if (p > i) {
+          bool up = ((i & k) == 0);
+          double a = key[i], b = key[p];
+          int ia = idx[i], ib = idx[p];
+          int sa = ia >> 28, sb = ib >> 28;
+          bool gt = (sa > sb) || (sa == sb && ((a > b) || (a == b && ia > ib)));
+          if (gt == up) { key[i] = b; key[p] = a; idx[i] = ib; idx[p] = ia; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Sector filter of apply_sector_filter (kriging.F90:1093-1154) in one pass:
+// among the candidates j < nk (all within dmax2, sector sec[j] < nsec), the
+// nmax nearest of every sector (all of them when fewer) are appended to
+// out[*nout ...].  One histogram of nsec x (NBIN / nsec) distance buckets
+// finds every sector's boundary bucket at once; the boundary buckets are
+// sorted together by (sector, d2, idx).  *tie is set when a sector's cut
+// falls between equal distances (the reference's heap order then decides:
+// the caller takes the exact kd-tree path); returns false when the boundary
+// buckets overflow bcap.
+__device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax, double dmax2, int bcap,
+                                    int* nout, bool* tie) {
+  const int lane = threadIdx.x & 31;
+  const int nbk = NBIN / nsec;                  // buckets per sector
+  const int lps = nbk / 8;                      // lanes per sector (8 bins per lane)
+  for (int i = lane; i < NBIN; i += 32) b.hist[i] = 0;
+  __syncwarp();
+  const double scale = dmax2 > 0.0 ? (double)nbk / dmax2 : 0.0;
+  for (int j = lane; j < nk; j += 32) {
+    int q = (int)(b.d2[j] * scale);
+    q = q < 0 ? 0 : (q >= nbk ? nbk - 1 : q);
+    atomicAdd(&b.hist[b.sec[j] * nbk + q], 1);
+  }
+  __syncwarp();
+  // segmented inclusive scan: lane owns bins 8 lane .. 8 lane + 7
+  int loc[8], sum = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) { loc[q] = b.hist[lane * 8 + q]; sum += loc[q]; }
+  const int seg = lane % lps;
+  int incl = sum;
+  for (int o = 1; o < lps; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (seg >= o) incl += t;
+  }
+  const int excl = incl - sum;
+  const int total = __shfl_sync(0xffffffffu, incl, (lane / lps) * lps + lps - 1);
+  __syncwarp();
+  // per sector: boundary bucket bs (nbk = none: the sector is taken whole)
+  // and the count below it; kept in hist[NBIN - 32 ..] after the scan
+  int* bsec = b.hist + NBIN - 32;   // [8] boundary bucket of each sector
+  int* cbel = b.hist + NBIN - 24;   // [8] count below the boundary
+  int* hb = b.hist + NBIN - 16;     // [8] size of the boundary bucket
+  int* fill = b.hist + NBIN - 8;    // [8] boundary fill cursors
+  const int sector = lane / lps;
+  if (seg == 0 && total <= nmax) { bsec[sector] = nbk; cbel[sector] = total; hb[sector] = 0; }
+  if (total > nmax && excl < nmax && incl >= nmax) {
+    int acc = excl;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      if (acc + loc[q] >= nmax) {
+        bsec[sector] = seg * 8 + q;
+        cbel[sector] = acc;
+        hb[sector] = loc[q];
+        break;
+      }
+      acc += loc[q];
+    }
+  }
+  __syncwarp();
+  // boundary segments: offsets by sector
+  int off[8];
+  int nbt = 0;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    off[s] = nbt;
+    if (s < nsec) nbt += hb[s];
+  }
+  if (nbt > bcap) return false;
+  if (lane < 8) fill[lane] = 0;
+  __syncwarp();
+  // pass 2: emit everything below the boundary buckets, collect those buckets
+  int no = *nout;
+  for (int base = 0; base < nk; base += 32) {
+    const int j = base + lane;
+    int sj = 0, q = 0, bs = 0;
+    if (j < nk) {
+      sj = b.sec[j];
+      q = (int)(b.d2[j] * scale);
+      q = q < 0 ? 0 : (q >= nbk ? nbk - 1 : q);
+      bs = bsec[sj];
+    }
+    const bool below = j < nk && q < bs;
+    const bool atb = j < nk && q == bs;
+    const unsigned lo = __ballot_sync(0xffffffffu, below);
+    if (below) b.out[no + __popc(lo & lanemask_lt())] = b.idx[j];
+    if (atb) {
+      int o2 = 0;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) if (s == sj) o2 = off[s];
+      const int p = o2 + atomicAdd(&fill[sj], 1);
+      b.bd2[p] = b.d2[j];
+      b.bidx[p] = b.idx[j] | (sj << 28);
+    }
+    no += __popc(lo);
+  }
+  __syncwarp();
+  bool t_any = false;
+  if (nbt > 0) {
+    int np2 = 32;
+    while (np2 < nbt) np2 <<= 1;
+    for (int i = nbt + lane; i < np2; i += 32) { b.bd2[i] = 1.0e308; b.bidx[i] = 0x7fffffff; }
+    __syncwarp();
+    warp_sort_sec(b.bd2, b.bidx, np2);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      if (s >= nsec || hb[s] == 0) continue;
+      const int r = nmax - cbel[s];
+      for (int i = lane; i < r; i += 32) b.out[no + i] = b.bidx[off[s] + i] & 0x0fffffff;
+      if (r < hb[s] && b.bd2[off[s] + r] == b.bd2[off[s] + r - 1]) t_any = true;
+      no += r;
+    }
+  }
+  *tie = t_any;
+  *nout = no;
+  __syncwarp();
+  return true;
+}
+
 // Per-warp candidate buffers of k_search: CAP candidates {d2, idx, sector},
 // OCAP selected, BCAP boundary-bucket entries and the 256-bin histogram.
 // Sized so that three 4-warp CTAs fit on an SM; a target whose ball holds
@@ -654,30 +794,10 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
           }
           const int nsec = 1 << S.ndim;
           int nfin = 0;
-          for (int s = 0; s < nsec; ++s) {
-            int cnt = 0;
-            for (int j = lane; j < nk; j += 32) cnt += (B.sec[j] == s);
-            for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            if (cnt == 0) continue;
-            if (cnt <= S.nmax) {
-              for (int base = 0; base < nk; base += 32) {
-                int j = base + lane;
-                bool in = j < nk && B.sec[j] == s;
-                unsigned m = __ballot_sync(0xffffffffu, in);
-                if (in) B.out[nfin + __popc(m & lanemask_lt())] = B.idx[j];
-                nfin += __popc(m);
-              }
-              __syncwarp();
-            } else {
-              double Ts;
-              bool ties = false;
-              int nf = nfin;
-              bool ok2 = warp_select(B, nk, S.nmax, T, BCAP, [&](int j) { return B.sec[j] == s; }, &nf, &Ts, &ties);
-              if (!ok2) st |= KK_ST_OVERFLOW;
-              if (ties) st |= KK_ST_TIE;
-              nfin = nf;
-            }
-          }
+          bool ties = false;
+          if (nsec * S.nmax >= OCAP || !warp_select_sectors(B, nk, nsec, S.nmax, T, BCAP, &nfin, &ties))
+            st |= KK_ST_OVERFLOW;
+          if (ties) st |= KK_ST_TIE;
           __syncwarp();
           for (int i = lane; i < nfin; i += 32) B.idx[i] = B.out[i];
           nsel = nfin;
