@@ -700,33 +700,62 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
       ylo = max(0, (int)floor((qg[1] - Dr - g.lo[1]) * g.inv_h[1]) - 1);
       yhi = min(g.n[1] - 1, (int)floor((qg[1] + Dr - g.lo[1]) * g.inv_h[1]) + 1);
     }
-    for (int z = zlo; z <= zhi && !overflow; ++z) {
-      double dz2 = 0.0;
-      if (g.G > 2) {
-        double zl = g.lo[2] + z * g.h[2] - 1e-6 * g.h[2], zh = zl + 1.000002 * g.h[2];
-        double dz = qg[2] < zl ? zl - qg[2] : (qg[2] > zh ? qg[2] - zh : 0.0);
-        dz2 = dz * dz;
-        if (dz2 > D2) continue;
-      }
-      for (int y = ylo; y <= yhi && !overflow; ++y) {
-        double dy2 = dz2;
-        if (g.G > 1) {
-          double yl = g.lo[1] + y * g.h[1] - 1e-6 * g.h[1], yh = yl + 1.000002 * g.h[1];
-          double dy = qg[1] < yl ? yl - qg[1] : (qg[1] > yh ? qg[1] - yh : 0.0);
-          dy2 += dy * dy;
-          if (dy2 > D2) continue;
+    // cell rows (y, z) that can meet the ball: lanes take 32 rows at a time
+    // and find each row's contiguous point range; the ranges of the group are
+    // then gathered 32 points at a time (a lane finds its row by bisection
+    // over the range starts), so short rows do not leave lanes idle
+    {
+      int* rstart = B.hist;       // [32] exclusive prefix of the range lengths
+      int* rp0 = B.hist + 32;     // [32] first sorted point of each row's range
+      const int ny = g.G > 1 ? yhi - ylo + 1 : 1;
+      const int nz = g.G > 2 ? zhi - zlo + 1 : 1;
+      const int nrows = (ny > 0 && nz > 0) ? ny * nz : 0;
+      for (int rg = 0; rg < nrows && !overflow; rg += 32) {
+        const int ridx = rg + lane;
+        int p0 = 0, len = 0;
+        if (ridx < nrows) {
+          const int y = ylo + ridx % ny, z = zlo + ridx / ny;
+          double dy2 = 0.0;
+          if (g.G > 2) {
+            double zl = g.lo[2] + z * g.h[2] - 1e-6 * g.h[2], zh = zl + 1.000002 * g.h[2];
+            double dz = qg[2] < zl ? zl - qg[2] : (qg[2] > zh ? qg[2] - zh : 0.0);
+            dy2 = dz * dz;
+          }
+          if (g.G > 1) {
+            double yl = g.lo[1] + y * g.h[1] - 1e-6 * g.h[1], yh = yl + 1.000002 * g.h[1];
+            double dy = qg[1] < yl ? yl - qg[1] : (qg[1] > yh ? qg[1] - yh : 0.0);
+            dy2 += dy * dy;
+          }
+          if (dy2 <= D2) {
+            double wx = sqrt(fmax(D2 - dy2, 0.0));
+            int x0 = max(0, (int)floor((qg[0] - wx - g.lo[0]) * g.inv_h[0]) - 1);
+            int x1 = min(g.n[0] - 1, (int)floor((qg[0] + wx - g.lo[0]) * g.inv_h[0]) + 1);
+            int row = (g.G > 1 ? y : 0) * g.n[0] + (g.G > 2 ? z * g.n[0] * g.n[1] : 0);
+            p0 = __ldg(&g.cell_start[row + x0]);
+            len = __ldg(&g.cell_start[row + x1 + 1]) - p0;
+          }
         }
-        double wx = sqrt(fmax(D2 - dy2, 0.0));
-        int x0 = max(0, (int)floor((qg[0] - wx - g.lo[0]) * g.inv_h[0]) - 1);
-        int x1 = min(g.n[0] - 1, (int)floor((qg[0] + wx - g.lo[0]) * g.inv_h[0]) + 1);
-        int row = (g.G > 1 ? y : 0) * g.n[0] + (g.G > 2 ? z * g.n[0] * g.n[1] : 0);
-        int p0 = __ldg(&g.cell_start[row + x0]);
-        int p1 = __ldg(&g.cell_start[row + x1 + 1]);
-        for (int base = p0; base < p1; base += 32) {
-          int j = base + lane;
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t2 = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t2;
+        }
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        rstart[lane] = incl - len;
+        rp0[lane] = p0;
+        __syncwarp();
+        for (int base = 0; base < tot; base += 32) {
+          const int i = base + lane;
+          int j = 0;
           double d2v = 0.0;
           bool in = false;
-          if (j < p1) {
+          if (i < tot) {
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+              if (rstart[k + step] <= i) k += step;
+            j = rp0[k] + (i - rstart[k]);
             d2v = dist2(g, q, j);
             in = d2v <= D2;
           }
@@ -747,6 +776,7 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
           M += __popc(m);
           if (M > CAP) overflow = true;
         }
+        __syncwarp();  // the next group reuses rstart / rp0
       }
     }
     __syncwarp();
