@@ -524,6 +524,12 @@ void engine_solve(Engine& e) {
   SolveParams P;
   fill_params(e, P);
   P.fast_model = (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_B) ? 1 : 0;
+  if (P.fast_model) {
+    for (int k = 0; k < 9; ++k) P.fm[k] = mdl[0].bmat[k];
+    P.fm_ndim = mdl[0].ndim;
+    P.fm_tail = mdl[0].btail;
+    P.fm_tab_off = mdl[0].btab_off;
+  }
 
   // ---- bucket by neighbour count
   timer.start();

@@ -49,7 +49,9 @@ struct SolveParams {
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
   double refine_tol_corr;    // bound on the FP32 correction term relative to its value
-  int fast_model;            // one variable, spatial, one Level-B table: register fast path
+  int fast_model;            // one variable, spatial, one Level-B table: fast covariance path
+  int fm_ndim, fm_tail, fm_tab_off;  // that model's dimension, analytic tail, table offset
+  double fm[9];              // and its anisotropy transform (bmat)
 };
 
 enum {

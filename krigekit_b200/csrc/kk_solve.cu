@@ -1055,7 +1055,7 @@ int solve_refine_form(const SolveParams& P, int precision) {
 
 void launch_assemble(const SolveParams& P, int N, const int* list, const int* cnt, int item0, int nitems,
                      double* Kg, int nsm, cudaStream_t st) {
-  int blocks = nsm * 4;
+  int blocks = nsm * 3;  // the launch bound's residency
   const int need = (nitems + 7) / 8;
   if (need < blocks) blocks = need > 0 ? need : 1;
   if (N == 32) k_assemble<32><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);

@@ -78,20 +78,11 @@ __device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, cons
   return dadd(t.x, dmul(fi, t.y));
 }
 
-// One Level-B model held in registers (single-variable spatial kriging):
-// COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past the table.
-struct FastModel {
-  double m[9];
-  const double2* tab;
-  const KkModel* model;
-  int ndim, tail;
-};
-
 // analytic tail past the last table zone (struct_cov_h), kept out of line so
-// that the rarely taken shape code does not raise the kernel's register count
+// that the rarely taken shape code does not raise the kernels' register count
 __device__ __noinline__ double tail_cov(const KkModel* m, double h) { return model_cov_h(*m, h); }
 
-// COV(vgm(first, second), lag) for models without a register fast path
+// COV(vgm(first, second), lag) for models without the fast path
 __device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, int second, const double* lag) {
   return cov_pair(P, first, second, lag);
 }
@@ -116,10 +107,14 @@ __device__ __forceinline__ double aniso_h_fast(const double* m, int ndim, const 
   return h2 > 0.0 ? h2 * rsqrt(h2) : 0.0;
 }
 
-__device__ __forceinline__ double fast_cov(const FastModel& f, const ZoneRegs& z, const double* lag) {
-  const double h = aniso_h_fast(f.m, f.ndim, lag);
-  if (h < z.zb3) return tab_fast(f.tab, z, h);
-  return f.tail ? tail_cov(f.model, h) : 0.0;
+// The single Level-B model of single-variable spatial kriging (P.fast_model):
+// COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past the table.
+// Its transform and table offset travel in the kernel parameters, which the
+// kernels read as uniform constant operands instead of holding registers.
+__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag) {
+  const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
+  if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off, z, h);
+  return P.fm_tail ? tail_cov(P.models, h) : 0.0;
 }
 
 template <typename T, int N, bool REFINE>
@@ -249,7 +244,7 @@ __device__ __forceinline__ int gather_rows(const SolveParams& P, int t, int lane
 // so it runs as its own kernel with many resident warps; the factorisation
 // kernel then reads K from this buffer (L2-resident in chunks).
 template <int N>
-__global__ void __launch_bounds__(256, 4) k_assemble(const __grid_constant__ SolveParams P,
+__global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ SolveParams P,
                                                      const int* __restrict__ list,
                                                      const int* __restrict__ list_count, int item0, int nitems,
                                                      double* __restrict__ Kg) {
@@ -266,16 +261,6 @@ __global__ void __launch_bounds__(256, 4) k_assemble(const __grid_constant__ Sol
   if (list_count) count = min(nitems, *list_count - item0);
   const bool fast = P.fast_model != 0;
   const ZoneRegs zr = load_zones();
-  FastModel fm;
-  if (fast) {
-    const KkModel& m0 = P.models[0];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) fm.m[k] = m0.bmat[k];
-    fm.tab = P.tables + m0.btab_off;
-    fm.model = &m0;
-    fm.ndim = m0.ndim;
-    fm.tail = m0.btail;
-  }
   const int nwarp = gridDim.x * (blockDim.x >> 5);
   for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < count; it += nwarp) {
     const int t = __ldg(&list[item0 + it]);
@@ -301,7 +286,7 @@ __global__ void __launch_bounds__(256, 4) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? fast_cov(fm, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
+        kv = fast ? fast_cov(P, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
       }
       K[e] = kv;
       c += 32;
@@ -346,16 +331,6 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   const int C = pa + q + nu;  // forward-substituted columns (FP64 form)
   const ZoneRegs zr = load_zones();
 
-  FastModel fm;
-  if (fast) {
-    const KkModel& m0 = P.models[0];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) fm.m[k] = m0.bmat[k];
-    fm.tab = P.tables + m0.btab_off;
-    fm.model = &m0;
-    fm.ndim = m0.ndim;
-    fm.tail = m0.btail;
-  }
 
   int n_chol = 0, n_iter = 0;
   for (;;) {
@@ -407,7 +382,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
 #pragma unroll
                 for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
               }
-              v = dadd(0.0, dmul(fast_cov(fm, zr, lag), 1.0));
+              v = dadd(0.0, dmul(fast_cov(P, zr, lag), 1.0));
             } else {
               v = rhs_cov_row(P, t, xr, vr, iv, rs);
             }
