@@ -1029,23 +1029,23 @@ static void launch_reg(const SolveParams& P, const int* list, const int* cnt, in
   k_solve_reg<T, NPAD, REFINE><<<nsm * occ, NPAD, 0, st>>>(P, list, cnt, slot);
 }
 
-template <typename T, int N, bool REFINE>
+template <typename T, int N, bool REFINE, int CB>
 static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
                         const double* Kg, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
   const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
   static bool attr_set = false;  // per instantiation
   if (!attr_set) {
-    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_set = true;
   }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE>, 32 * WPC, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE, CB>, 32 * WPC, smem);
   if (occ < 1) occ = 1;
   int blocks = nsm * occ;
   const int need = (nitems + WPC - 1) / WPC;
   if (need < blocks) blocks = need > 0 ? need : 1;
-  k_solve_warp<T, N, REFINE><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
+  k_solve_warp<T, N, REFINE, CB><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
 }
 
 int solve_refine_form(const SolveParams& P, int precision) {
@@ -1064,12 +1064,24 @@ void launch_assemble(const SolveParams& P, int N, const int* list, const int* cn
 
 void launch_factor(const SolveParams& P, int refine, int N, const int* list, const int* cnt, int item0, int nitems,
                    const double* Kg, int slot, int nsm, cudaStream_t st) {
+  const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
+  const bool narrow = C <= 3;
   if (refine) {
-    if (N == 32) launch_warp<float, 32, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
-    else launch_warp<float, 64, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    if (N == 32) {
+      if (narrow) launch_warp<float, 32, true, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<float, 32, true, KK_REFINE_COLS>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    } else {
+      if (narrow) launch_warp<float, 64, true, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<float, 64, true, KK_REFINE_COLS>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    }
   } else {
-    if (N == 32) launch_warp<double, 32, false>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
-    else launch_warp<double, 64, false>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    if (N == 32) {
+      if (narrow) launch_warp<double, 32, false, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<double, 32, false, MAXC>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    } else {
+      if (narrow) launch_warp<double, 64, false, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<double, 64, false, MAXC>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    }
   }
 }
 

@@ -301,19 +301,22 @@ template <typename T, int N, bool REFINE>
 constexpr int warp_cta() { return 4; }
 
 // CTAs per SM the register budget is sized for (the launch bound caps the
-// registers at 64 K / (threads * this)): the N = 64 forms need the whole
-// register file of a lane for the matrix, the N = 32 forms fit in 128
+// registers at 64 K / (threads * this)): the FP64 N = 64 form needs the whole
+// register file of a lane for the matrix, the FP32 one fits in 168, the
+// N = 32 forms in 128
 template <typename T, int N, bool REFINE>
-constexpr int warp_min_ctas() { return N == 64 ? 1 : 4; }
+constexpr int warp_min_ctas() { return N == 64 ? (REFINE ? 3 : 1) : 4; }
 
-template <typename T, int N, bool REFINE>
+// CB: right-hand-side columns held per row at compile time (F | k | u);
+// 3 covers ordinary and simple kriging of one variable, the wider forms
+// cover drift and cokriging.
+template <typename T, int N, bool REFINE, int CB>
 __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE>())
     k_solve_warp(const __grid_constant__ SolveParams P, const int* __restrict__ list,
                  const int* __restrict__ list_count, int item0, int nitems, const double* __restrict__ Kg,
                  int work_slot) {
   using WS = WarpSmem<T, N, REFINE>;
   constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
-  constexpr int CB = REFINE ? KK_REFINE_COLS : MAXC;  // right-hand-side columns held per row
   // column-buffer row stride: padded so the four row classes fall in
   // different banks and stay 16-byte aligned
   constexpr int RIP = RI + (sizeof(T) == 8 ? 2 : 4);
@@ -506,10 +509,10 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
     if constexpr (!REFINE) {
       // ---- G = Y^T Y over the forward-substituted columns
 #pragma unroll
-      for (int ka = 0; ka < MAXC; ++ka) {
+      for (int ka = 0; ka < CB; ++ka) {
         if (ka >= C) break;
 #pragma unroll
-        for (int kb = ka; kb < MAXC; ++kb) {
+        for (int kb = ka; kb < CB; ++kb) {
           if (kb >= C) break;
           double g = 0.0;
 #pragma unroll
