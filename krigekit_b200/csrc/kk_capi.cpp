@@ -53,6 +53,12 @@ static Engine* get(int64_t h) {
 
 static int ierr() { return failed() ? 1 : 0; }
 
+// device -> host copy of solve results, with the CUDA status checked
+static void copy_d2h(void* dst, const void* src, size_t bytes) {
+  const cudaError_t err = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+  if (err != cudaSuccess) throw std::string("CUDA error ") + cudaGetErrorString(err) + " reading results";
+}
+
 static int vtype_id(const char* s) {
   // vtype_from_str, vgmfunc.f90:83-99 (case-insensitive 3-character prefix)
   static const char* names[] = {"nug", "sph", "exp", "gau", "hol", "pow", "bsq", "cir", "lin", "cyc", "dco"};
@@ -168,28 +174,40 @@ int krige_set_obs(int64_t h, int ivar, int nobs, int ndim_c, const double* coord
   o.value.assign(value, value + nobs);
   if (variance) o.variance.assign(variance, variance + nobs);
   else o.variance.assign(nobs, 0.0);
-  // duplicate coordinate check (check_duplicate_coordinates_base, utils.F90:43-133)
+  // duplicate coordinate check (check_duplicate_coordinates_base, utils.F90:43-133):
+  // open-addressing hash table over all coordinates, full comparison on a
+  // matching slot (equal coordinates always hash alike)
   {
-    std::vector<int> idx(nobs);
-    for (int i = 0; i < nobs; ++i) idx[i] = i;
     const double* c = o.coord.data();
-    std::sort(idx.begin(), idx.end(), [&](int a, int b) {
+    size_t cap = 1;
+    while (cap < 2 * (size_t)nobs + 2) cap <<= 1;
+    std::vector<int> slot(cap, -1);
+    for (int i = 0; i < nobs; ++i) {
+      uint64_t hsh = 0x9e3779b97f4a7c15ull;
       for (int k = 0; k < ndim_c; ++k) {
-        double x = c[(size_t)a * ndim_c + k], y = c[(size_t)b * ndim_c + k];
-        if (x != y) return x < y;
+        double v = c[(size_t)i * ndim_c + k];
+        if (v == 0.0) v = 0.0;  // -0.0 and 0.0 are the same coordinate
+        uint64_t bits;
+        std::memcpy(&bits, &v, sizeof bits);
+        hsh ^= bits + 0x9e3779b97f4a7c15ull + (hsh << 6) + (hsh >> 2);
+        hsh *= 0xff51afd7ed558ccdull;
+        hsh ^= hsh >> 33;
       }
-      return a < b;
-    });
-    for (int i = 1; i < nobs; ++i) {
-      bool same = true;
-      for (int k = 0; k < ndim_c; ++k)
-        if (c[(size_t)idx[i] * ndim_c + k] != c[(size_t)idx[i - 1] * ndim_c + k]) { same = false; break; }
-      if (same) {
-        char msg[160];
-        snprintf(msg, sizeof msg, "Duplicate observation coordinates at points %d and %d", idx[i - 1] + 1, idx[i] + 1);
-        o = ObsVar();
-        throw std::string(msg);
+      size_t p = hsh & (cap - 1);
+      while (slot[p] >= 0) {
+        const int j = slot[p];
+        bool same = true;
+        for (int k = 0; k < ndim_c; ++k)
+          if (c[(size_t)i * ndim_c + k] != c[(size_t)j * ndim_c + k]) { same = false; break; }
+        if (same) {
+          char msg[160];
+          snprintf(msg, sizeof msg, "Duplicate observation coordinates at points %d and %d", j + 1, i + 1);
+          o = ObsVar();
+          throw std::string(msg);
+        }
+        p = (p + 1) & (cap - 1);
       }
+      slot[p] = i;
     }
   }
   o.nmax = nmax;
@@ -495,12 +513,21 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
   if (!e) return 1;
   check_solved(e);
   const int nv = e->nvar;
-  std::vector<double> tmp((size_t)e->nblock * nv);
-  cudaMemcpy(tmp.data(), e->est.p, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost);
-  for (int is = 0; is < nsim_c; ++is)
+  if (nblocks < 0 || nblocks > e->nblock || nvar_c < 0 || nvar_c > nv || nsim_c < 0)
+    throw std::string("output dimensions exceed the solved blocks or variables");
+  if (nblocks == 0 || nvar_c == 0 || nsim_c == 0) return 0;
+  if (nv == 1) {
+    // est is (nblock) on the device: copy the first column straight into out
+    copy_d2h(out, e->est.p, sizeof(double) * nblocks);
+  } else {
+    std::vector<double> tmp((size_t)e->nblock * nv);
+    copy_d2h(tmp.data(), e->est.p, sizeof(double) * tmp.size());
     for (int iv = 0; iv < nvar_c; ++iv)
-      for (int ib = 0; ib < nblocks; ++ib)
-        out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * is)] = tmp[(size_t)ib * nv + iv];
+      for (int ib = 0; ib < nblocks; ++ib) out[ib + (size_t)nblocks * iv] = tmp[(size_t)ib * nv + iv];
+  }
+  // every realisation slot holds the kriging estimate (no simulation)
+  for (int is = 1; is < nsim_c; ++is)
+    std::memcpy(out + (size_t)nblocks * nvar_c * is, out, sizeof(double) * (size_t)nblocks * nvar_c);
   KK_GUARD_END
 }
 
@@ -516,12 +543,19 @@ int krige_get_variance_all(int64_t h, int nblocks, int nvar_c, double* out) {
   if (!e) return 1;
   check_solved(e);
   const int nv = e->nvar;
-  std::vector<double> tmp((size_t)e->nblock * nv * nv);
-  cudaMemcpy(tmp.data(), e->var.p, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost);
-  for (int jv = 0; jv < nvar_c; ++jv)
-    for (int iv = 0; iv < nvar_c; ++iv)
-      for (int ib = 0; ib < nblocks; ++ib)
-        out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * jv)] = tmp[(size_t)ib * nv * nv + iv + (size_t)jv * nv];
+  if (nblocks < 0 || nblocks > e->nblock || nvar_c < 0 || nvar_c > nv)
+    throw std::string("output dimensions exceed the solved blocks or variables");
+  if (nblocks == 0 || nvar_c == 0) return 0;
+  if (nv == 1) {
+    copy_d2h(out, e->var.p, sizeof(double) * nblocks);
+  } else {
+    std::vector<double> tmp((size_t)e->nblock * nv * nv);
+    copy_d2h(tmp.data(), e->var.p, sizeof(double) * tmp.size());
+    for (int jv = 0; jv < nvar_c; ++jv)
+      for (int iv = 0; iv < nvar_c; ++iv)
+        for (int ib = 0; ib < nblocks; ++ib)
+          out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * jv)] = tmp[(size_t)ib * nv * nv + iv + (size_t)jv * nv];
+  }
   KK_GUARD_END
 }
 
@@ -573,8 +607,8 @@ int krige_get_neighbours(int64_t h, int ivar, int nblocks, int mmax, int* nnear,
   VarDevice& d = e->vd[ivar - 1];
   const int mm = std::max(d.search.mmax, 1);
   std::vector<int> nn(e->nblock), nb((size_t)e->nblock * mm);
-  cudaMemcpy(nn.data(), d.nnear.p, sizeof(int) * nn.size(), cudaMemcpyDeviceToHost);
-  cudaMemcpy(nb.data(), d.nbr.p, sizeof(int) * nb.size(), cudaMemcpyDeviceToHost);
+  copy_d2h(nn.data(), d.nnear.p, sizeof(int) * nn.size());
+  copy_d2h(nb.data(), d.nbr.p, sizeof(int) * nb.size());
   for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib) {
     nnear[ib] = nn[ib];
     for (int k = 0; k < mmax; ++k) inear[(size_t)ib * mmax + k] = (k < nn[ib] && k < mm) ? nb[(size_t)ib * mm + k] + 1 : 0;
@@ -598,7 +632,7 @@ int krige_get_status(int64_t h, int nblocks, int* status) {
   if (!e) return 1;
   check_solved(e);
   std::vector<int> s(e->nblock);
-  cudaMemcpy(s.data(), e->status.p, sizeof(int) * s.size(), cudaMemcpyDeviceToHost);
+  copy_d2h(s.data(), e->status.p, sizeof(int) * s.size());
   for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib) status[ib] = s[ib];
   KK_GUARD_END
 }

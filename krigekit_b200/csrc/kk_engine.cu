@@ -446,11 +446,19 @@ void engine_solve(Engine& e) {
 
   // ---- targets
   if (e.grid_dirty) {
-    std::vector<double> tmp(nb);
-    for (int k = 0; k < D; ++k) {
-      for (int i = 0; i < nb; ++i) tmp[i] = e.bcoord[(size_t)i * D + k];
-      upload(e.tx[k], tmp.data(), sizeof(double) * nb, st);
+    // target coordinates: transposed into pinned staging, one copy per axis
+    const size_t need = sizeof(double) * (size_t)nb * D;
+    if (e.hstage_bytes < need) {
+      if (e.hstage) cudaFreeHost(e.hstage);
+      e.hstage = nullptr;
+      e.hstage_bytes = 0;
+      KK_CUDA(cudaMallocHost(&e.hstage, need));
+      e.hstage_bytes = need;
     }
+    double* hs = static_cast<double*>(e.hstage);
+    for (int i = 0; i < nb; ++i)
+      for (int k = 0; k < D; ++k) hs[(size_t)k * nb + i] = e.bcoord[(size_t)i * D + k];
+    for (int k = 0; k < D; ++k) upload(e.tx[k], hs + (size_t)k * nb, sizeof(double) * nb, st);
     for (int k = D; k < 4; ++k) e.tx[k].reserve(8);
     if (!e.rangescale.empty()) upload(e.trs, e.rangescale.data(), sizeof(double) * nb, st);
     if (!e.localnugget.empty()) upload(e.tln, e.localnugget.data(), sizeof(double) * nb, st);
@@ -678,6 +686,9 @@ void engine_release(Engine& e) {
   e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
   e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
   e.counters.release(); e.scratch.release(); e.kbuf.release();
+  if (e.hstage) cudaFreeHost(e.hstage);
+  e.hstage = nullptr;
+  e.hstage_bytes = 0;
 }
 
 }  // namespace kk

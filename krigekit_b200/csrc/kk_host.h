@@ -93,6 +93,8 @@ struct Engine {
   DBuf models, tables, tx[4], trs, tln, tdrift, gstart, gx[4], gw;
   DBuf est, var, status, npp, bucket, counters, scratch;
   DBuf kbuf;  // packed K64 of one chunk of targets (assembly -> factorisation)
+  void* hstage = nullptr;  // pinned host staging for target uploads
+  size_t hstage_bytes = 0;
   size_t scratch_bytes = 0;
   int mmax_total = 0;
   bool solved = false;

@@ -155,11 +155,11 @@ class Kriging:
             if var_f.size != nobs:
                 raise ValueError(f"variance length ({var_f.size}) must match nobs ({nobs})")
         else:
-            var_f = _farray(np.zeros(nobs))
+            var_f = None  # zero measurement variance
         c_nmax = int(nmax) if nmax is not None else np.iinfo(np.int32).max
         c_maxdist = float(maxdist) if maxdist is not None else sys.float_info.max
         _lib.call("krige_set_obs", self._h(), ivar, nobs, ndim_c, _dptr(coord_f), _dptr(value_f),
-                  _dptr(var_f), c_nmax, c_maxdist, float(sk_mean))
+                  None if var_f is None else _dptr(var_f), c_nmax, c_maxdist, float(sk_mean))
         self._nobs[ivar - 1] = nobs
 
     def set_obs_drift(self, ivar: int, drift):
@@ -202,9 +202,11 @@ class Kriging:
             return
         coord_f = _coord_to_fortran(coord)
         ngrid = coord_f.shape[1]
-        rs_f = _farray(rangescale) if rangescale is not None else _farray(np.ones(ngrid))
-        ln_f = _farray(localnugget) if localnugget is not None else _farray(np.zeros(ngrid))
-        _lib.call("krige_set_grid", self._h(), ngrid, coord_f.shape[0], _dptr(coord_f), _dptr(rs_f), _dptr(ln_f))
+        # absent rangescale / localnugget: null (all ones / zeros in the library)
+        rs_f = _farray(rangescale) if rangescale is not None else None
+        ln_f = _farray(localnugget) if localnugget is not None else None
+        _lib.call("krige_set_grid", self._h(), ngrid, coord_f.shape[0], _dptr(coord_f),
+                  None if rs_f is None else _dptr(rs_f), None if ln_f is None else _dptr(ln_f))
         self._nblock = ngrid
 
     def set_grid_block(self, coord, block_type: int, nblockpnt=None, pointweight=None, blocksize=None,
