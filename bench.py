@@ -2,7 +2,10 @@
 """Benchmark: kriged targets/s on one B200 for the 2-D anisotropic sector-search
 ordinary-kriging workload (200 000 clustered observations, 2000 x 2000 targets).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
+
+``--config`` picks one of the five workloads of bench_workloads.py at its full
+size (default 2, the benchmark); the JSON line has the same keys for each.
 
 Prints one JSON line.  ``value`` is device throughput of the FP32-factor +
 FP64-refinement form with inputs resident in HBM (CUDA events on the solve
@@ -139,53 +142,65 @@ def hbm_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def cpu_sample_run(w, nthread, target_seconds, precision_ref=None):
+def cpu_sample_run(W, nthread, target_seconds):
     """Time the CPU oracle on a contiguous slab of targets (all observations)."""
-    from oracle.oracle import OracleKriging
-    grid = w["grid"]
 
     def run(lo, hi):
-        o = OracleKriging(ndim=w["ndim"], nvar=w["nvar"], nmin=w.get("nmin", 0), **w["kw"])
-        bw.apply(o, w, set_grid=False)
-        o.set_grid(grid[lo:hi])
+        o = W.oracle(idx=np.arange(lo, hi))
         t0 = time.perf_counter()
         o.solve(nthread=nthread)
         return time.perf_counter() - t0, o
 
-    pilot = min(len(grid), 4000)
-    lo0 = (len(grid) // 2) - (len(grid) // 2) % 2000
+    n_all = W.ntarget
+    pilot = min(n_all, 4000)
+    lo0 = (n_all // 2) - (n_all // 2) % 2000
+    lo0 = min(lo0, n_all - pilot)
     dt, _ = run(lo0, lo0 + pilot)
     rate = pilot / max(dt, 1e-6)
-    n = int(min(len(grid) - lo0, max(pilot, rate * target_seconds)))
+    n = int(min(n_all - lo0, max(pilot, rate * target_seconds)))
     dt, o = run(lo0, lo0 + n)
     return dict(rate=n / dt, seconds=dt, lo=lo0, hi=lo0 + n, oracle=o)
 
 
-def run_reference(args, w):
+def workload_config(W):
+    w = W.w
+    vg = "; ".join(f"{i}{j} {s['vtype']} nug{s.get('nugget', 0)} sill{s.get('sill', 0)} a{s.get('a_major', '')}"
+                   for (i, j, s) in w["vgm"])
+    return {"workload": W.name, "ntargets": W.ntarget, "nobs": W.nobs, "ndim": w["ndim"], "nvar": w["nvar"],
+            "search": W.describe(), "variogram": vg}
+
+
+def run_reference(args, W):
     nthread = os.cpu_count() or 1
     step_rates = []
     for _ in range(args.warmup):
-        cpu_sample_run(w, nthread, args.cpu_seconds / 4)
+        cpu_sample_run(W, nthread, args.cpu_seconds / 4)
     last = None
     for _ in range(args.steps):
-        r = cpu_sample_run(w, nthread, args.cpu_seconds)
+        r = cpu_sample_run(W, nthread, args.cpu_seconds)
         step_rates.append(r["rate"])
         last = r
     value = statistics.median(step_rates)
-    sample = (f"targets {last['lo']}..{last['hi']} (rows of the 2000x2000 grid) with all "
-              f"{len(w['obs'][0]['coord'])} observations; {last['seconds']:.1f} s per step")
+    sample = (f"targets {last['lo']}..{last['hi']} of the {W.ntarget} targets with all "
+              f"{W.nobs} observations; {last['seconds']:.1f} s per step")
+    cfg = workload_config(W)
+    cfg["precision"] = "fp64"
     line = {
         "metric": METRIC, "value": value, "unit": "targets/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": last["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, see bench_workloads.py)",
-        "config": {"workload": w["name"], "ntargets": int(len(w["grid"])),
-                   "nobs": int(len(w["obs"][0]["coord"])), "precision": "fp64"},
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": "targets/s", "cores": nthread, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def neighbours(k, nvar):
+    """[(nnear, inear)] of each variable of the last solve."""
+    return [k.get_neighbours(iv) for iv in range(1, nvar + 1)]
 
 
 def main():
@@ -194,7 +209,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--grid", type=int, default=2000, help="targets per axis (default: the benchmark's 2000)")
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                    help="workload: 1 OK 2-D, 2 anisotropic sector OK (the benchmark), 3 KED 3-D, "
+                         "4 LMC cokriging, 5 space-time product-sum with block support")
+    ap.add_argument("--grid", type=int, default=None,
+                    help="targets per axis (default: the workload's own size, 2000 for the benchmark)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -209,8 +228,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        w = bw.config2(grid_n=args.grid)
-        run_reference(args, w)
+        run_reference(args, bw.Workload(args.config, args.grid))
         return
 
     import torch
@@ -223,11 +241,12 @@ def main():
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
-    from krigekit_b200 import Kriging
 
-    w = bw.config2(grid_n=args.grid)
-    ntarget = len(w["grid"])
-    nobs = len(w["obs"][0]["coord"])
+    W = bw.Workload(args.config, args.grid)
+    w = W.w
+    nvar = w["nvar"]
+    ntarget = W.ntarget
+    nobs = W.nobs
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def barrier():
@@ -259,19 +278,13 @@ def main():
         return tot, times
 
     # targets are sharded, never exchanged: rank r solves slab r of a global
-    # target set of world copies of the grid (weak scaling, fixed work per GPU)
+    # target set of world copies of the targets (weak scaling, fixed work per GPU)
     from krigekit_b200.shard import target_slab
     lo, hi = target_slab(world * ntarget, rank, world)
-    slab = w["grid"][np.arange(lo, hi) % ntarget]
-
-    def make(precision):
-        k = Kriging(ndim=2, nvar=1, precision=precision, nmin=w["nmin"], **w["kw"])
-        bw.apply(k, w, set_grid=False)
-        k.set_grid(slab)
-        return k
+    slab = np.arange(lo, hi) % ntarget
 
     # ---- FP32 + refinement (the measured form)
-    k32 = make(args.precision)
+    k32 = W.product(args.precision, idx=slab)
     sampler = ClockSampler(dev)
     tot32, times32 = time_steps(k32, args.steps, args.warmup, sampler)
     value = ntarget * world * args.steps / tot32
@@ -284,12 +297,13 @@ def main():
     k32.profile(False)
     gst = k32.gpu_stats()
     e32, v32 = k32.get_results()
-    nnear, _ = k32.get_neighbours(1)
+    nb32 = neighbours(k32, nvar)
+    nnear = sum(nn.astype(np.int64) for nn, _ in nb32)
 
     # ---- FP64 plain
     fp64 = None
     if not args.no_fp64 and args.precision != "fp64":
-        k64 = make("fp64")
+        k64 = W.product("fp64", idx=slab)
         tot64, _ = time_steps(k64, args.steps, args.warmup)
         k64.profile(True)
         flush.fill_(1.0)
@@ -300,7 +314,7 @@ def main():
                 "phases_ms": ph64}
         ee = bw.rel_err(e32, e64, 1e-3 * w["zstd"])
         ve = bw.rel_err(v32, v64, 1e-3 * w["sill"])
-        fin = np.isfinite(e64)
+        fin = np.isfinite(np.asarray(e64, dtype=np.float64))
         fp64["fp32_vs_fp64_rel_err"] = {
             "est_max": float(ee[fin].max()), "est_p99": float(np.percentile(ee[fin], 99)),
             "var_max": float(ve[fin].max()), "var_p99": float(np.percentile(ve[fin], 99))}
@@ -308,50 +322,52 @@ def main():
 
     # ---- roofline of the dominant kernel (the FP32 solve kernels)
     peaks = measured_peaks(torch, dev)
+    p_aug, q_rhs = W.pq()
     nn = nnear[nnear >= 2].astype(np.float64)
-    flops = float(solve_flops(nn).sum())
+    flops = float(solve_flops(nn, p_aug, q_rhs).sum())
     achieved = flops / (ph32["solve_ms"] / 1e3) / 1e12
     hbm_gbs, hbm_src = hbm_peak()
-    # search: algorithmic bytes = target coords + neighbour gathers (8*(ndim+1) per neighbour) + list write
-    search_bytes = ntarget * 16 + float(nn.sum()) * (8 * 3 + 4) + ntarget * 4
+    # search: algorithmic bytes = target coords + neighbour gathers (8*(coords+1) per neighbour) + list write
+    ncoord = w["ndim"] + (1 if W.st else 0)
+    search_bytes = len(slab) * 8 * ncoord + float(nn.sum()) * (8 * (ncoord + 1) + 4) + len(slab) * 4 * nvar
     search_gbs = search_bytes / (ph32["search_ms"] / 1e3) / 1e9
+    ncu_known = args.config == 2 and args.grid in (None, 2000)
 
     # ---- CPU baseline (oracle on a bounded sample) + accuracy against it
     cpu = None
     acc = None
     if rank == 0 and not args.no_cpu:
-        r = cpu_sample_run(w, os.cpu_count() or 1, args.cpu_seconds)
+        r = cpu_sample_run(W, os.cpu_count() or 1, args.cpu_seconds)
         o = r["oracle"]
         lo, hi = r["lo"], r["hi"]
         oe, ov = o.get_results()
-        ee = bw.rel_err(e32[lo:hi], oe, 1e-3 * w["zstd"])
-        ve = bw.rel_err(v32[lo:hi], ov, 1e-3 * w["sill"])
-        _, inear32 = k32.get_neighbours(1)
-        same = bool(np.array_equal(nnear[lo:hi], o.nnear[:, 0]))
-        if same:
-            m = inear32.shape[1]
-            same = bool(np.array_equal(inear32[lo:hi, :m], o.inear[:, 0, :m]))
+        ee = bw.rel_err(np.asarray(e32)[lo:hi], oe, 1e-3 * w["zstd"])
+        ve = bw.rel_err(np.asarray(v32)[lo:hi], ov, 1e-3 * w["sill"])
+        same = True
+        for iv, (nn_g, in_g) in enumerate(nb32):
+            same = same and bool(np.array_equal(nn_g[lo:hi], o.nnear[:, iv]))
+            if same:
+                m = min(in_g.shape[1], o.inear.shape[2])
+                same = bool(np.array_equal(in_g[lo:hi, :m], o.inear[:, iv, :m]))
         acc = {"vs_oracle_sample": f"targets {lo}..{hi}", "est_max": float(ee.max()),
                "est_p99": float(np.percentile(ee, 99)), "var_max": float(ve.max()),
                "var_p99": float(np.percentile(ve, 99)), "neighbour_sets_identical": same}
         cpu = {"value": r["rate"], "unit": "targets/s", "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": f"targets {lo}..{hi} of the 2000x2000 grid, all {nobs} observations, "
+               "sample": f"targets {lo}..{hi} of the {ntarget} targets, all {nobs} observations, "
                          f"{r['seconds']:.1f} s (oracle/kk_oracle.c, OpenMP dynamic,1, 64-slot factor cache)"}
 
     # ---- end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
-        obs = w["obs"][0]
-        k = Kriging(ndim=2, nvar=1, precision="fp32_refine", nmin=w["nmin"], **w["kw"])
-        for (i, j, spec) in w["vgm"]:
-            k.set_vgm(i, j, **spec)
+        k = W.product("fp32_refine", idx=slab)
+        io = {}
 
         def e2e_step():
-            k.set_obs(1, obs["coord"], obs["value"], nmax=obs["nmax"])
-            k.set_grid(w["grid"])
-            k.set_search(1, **w["search"][0])
+            io["h2d"] = W.set_data(k, slab)
             k.solve()
-            return k.get_results()
+            est, var = k.get_results()
+            io["d2h"] = np.asarray(est).nbytes + np.asarray(var).nbytes
+            return est, var
 
         for _ in range(max(1, args.warmup - 1)):
             e2e_step()
@@ -365,37 +381,37 @@ def main():
             t = torch.tensor([te], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             te = float(t.item())
-        h2d = nobs * (2 * 8 + 8 + 8) + ntarget * 2 * 8
-        d2h = ntarget * 8 * 2
         e2e = {"value": ntarget * world * args.steps / te, "unit": "targets/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "h2d_bytes_per_step": int(io["h2d"]), "d2h_bytes_per_step": int(io["d2h"]),
                "ms_per_step": te / args.steps * 1e3,
-               "note": "pageable numpy inputs through Kriging.set_obs/set_grid/solve/get_results"}
+               "note": "pageable numpy inputs through set_obs/set_grid/set_search/solve/get_results"}
+        del k
 
     if rank == 0:
+        cfg = workload_config(W)
+        cfg.update({"precision": args.precision, "l2": "flushed (256 MiB write) between timed steps",
+                    "parallelism": f"targets sharded per rank, {ntarget} per GPU (weak), {world} GPU(s)"})
         line = {
             "metric": METRIC, "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot32 / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 factor + f64 refinement" if args.precision == "fp32_refine" else "f64",
             "data": "synthetic (seeded, see bench_workloads.py)",
-            "config": {"workload": w["name"], "ntargets": ntarget, "nobs": nobs,
-                       "search": "anisotropic (0.5, az 30), 4 sectors x 16", "variogram": "exp r0.1 nug0.02",
-                       "precision": args.precision, "l2": "flushed (256 MiB write) between timed steps",
-                       "parallelism": f"targets sharded per rank, {ntarget} per GPU (weak), {world} GPU(s)"},
+            "config": cfg,
             "fp64_plain": fp64,
             "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "accuracy": acc,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
                          "frac": achieved / peaks["fp32"],
-                         "traffic": NCU_DRAM_BYTES_PER_TARGET["solve_fp32_refine"] * ntarget,
-                         "traffic_note": "ncu DRAM bytes per target (400x400 grid) x targets per launch",
+                         "traffic": NCU_DRAM_BYTES_PER_TARGET["solve_fp32_refine"] * ntarget if ncu_known else None,
+                         "traffic_note": ("ncu DRAM bytes per target (400x400 grid) x targets per launch"
+                                          if ncu_known else "no ncu capture of this workload"),
                          "kernel": "k_solve_warp<float,32|64,refine> (solve phase, CUDA-core FP32)",
                          "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live",
                          "flops_per_solve": flops, "solve_ms": ph32["solve_ms"]},
             "roofline_search": {"bound": "hbm", "achieved": search_gbs, "peak": hbm_gbs, "unit": "GB/s",
                                 "frac": search_gbs / hbm_gbs,
-                                "traffic": NCU_DRAM_BYTES_PER_TARGET["search"] * ntarget,
+                                "traffic": NCU_DRAM_BYTES_PER_TARGET["search"] * ntarget if ncu_known else None,
                                 "kernel": "k_search<768>", "peak_source": hbm_src,
                                 "search_ms": ph32["search_ms"]},
             "peaks_measured_tflops": peaks,

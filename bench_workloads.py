@@ -167,18 +167,14 @@ def st_blocks(w, pad3d=False):
     nbp = np.where(blk, 16, 1).astype(np.int32)
     ox, oy = np.meshgrid(GQ4_FRAC * cell, GQ4_FRAC * cell, indexing="ij")
     wq = np.outer(GQ4_W, GQ4_W).ravel()
-    nodes, ntime, wts = [], [], []
-    for i in range(len(g)):
-        if blk[i]:
-            xy = np.column_stack([g[i, 0] + ox.ravel(), g[i, 1] + oy.ravel()])
-            nodes.append(xy)
-            ntime.append(np.full(16, g[i, nd]))
-            wts.append(wq)
-        else:
-            nodes.append(g[i:i + 1, :2])
-            ntime.append(g[i:i + 1, nd])
-            wts.append(np.ones(1))
-    nodes, ntime, wts = np.vstack(nodes), np.concatenate(ntime), np.concatenate(wts)
+    owner = np.repeat(np.arange(len(g)), nbp)          # target of each node, in target order
+    within = np.arange(len(owner)) - np.repeat(np.cumsum(nbp) - nbp, nbp)
+    isb = blk[owner]
+    nodes = g[owner, :2].copy()
+    nodes[isb, 0] += ox.ravel()[within[isb]]
+    nodes[isb, 1] += oy.ravel()[within[isb]]
+    ntime = g[owner, nd]
+    wts = np.where(isb, wq[np.where(isb, within, 0)], 1.0)
     coord = g[:, :nd]
     if pad3d:
         coord = np.column_stack([coord, np.zeros(len(coord))])
@@ -186,7 +182,7 @@ def st_blocks(w, pad3d=False):
     return dict(coord=coord, time=g[:, nd], nblockpnt=nbp, node_coord=nodes, node_time=ntime, weight=wts)
 
 
-def apply_st(k, w, blocks=True, pad3d=False):
+def apply_st(k, w, blocks=True, pad3d=False, set_grid=True):
     """Configure a space-time kriging object (product or oracle) from a config-5 workload."""
     m = w["st_model"]
     k.set_st_model(model=m["model"], transform=m["transform"], at=m["at"], k_ps=m["k_ps"])
@@ -199,17 +195,148 @@ def apply_st(k, w, blocks=True, pad3d=False):
         k.set_vgm(i, j, **spec)
     for (i, j, spec) in w["vgm_t"]:
         k.set_vgm_temporal(i, j, **spec)
-    b = st_blocks(w, pad3d)
-    if blocks:
-        if hasattr(k, "set_grid_nodes"):
-            k.set_grid_nodes(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
+    if set_grid:
+        b = st_blocks(w, pad3d)
+        if blocks:
+            set_st_blocks(k, b)
         else:
-            k.set_grid_block(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
-    else:
-        k.set_grid(b["coord"], time=b["time"])
+            k.set_grid(b["coord"], time=b["time"])
     for iv, s in enumerate(w["search"], start=1):
         k.set_search(iv, **s)
     return k
+
+
+def set_st_blocks(k, b):
+    """Block targets on a product (set_grid_block) or oracle (set_grid_nodes) object."""
+    if hasattr(k, "set_grid_nodes"):
+        k.set_grid_nodes(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
+    else:
+        k.set_grid_block(b["coord"], b["time"], b["nblockpnt"], b["node_coord"], b["node_time"], b["weight"])
+
+
+def st_block_subset(b, idx):
+    """The blocks idx (and their nodes) of a st_blocks() dict."""
+    idx = np.asarray(idx)
+    nbp = b["nblockpnt"]
+    start = np.concatenate([[0], np.cumsum(nbp)[:-1]])
+    cnt = nbp[idx]
+    first = np.repeat(start[idx], cnt)
+    within = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    nodes = first + within
+    return dict(coord=b["coord"][idx], time=b["time"][idx], nblockpnt=cnt.astype(np.int32),
+                node_coord=b["node_coord"][nodes], node_time=b["node_time"][nodes], weight=b["weight"][nodes])
+
+
+class Workload:
+    """One configuration at a given size, configured onto the product classes
+    or the CPU oracle for any subset of its targets."""
+
+    def __init__(self, c, grid=None):
+        self.c = c
+        if c == 1:
+            self.w = config1(grid_n=grid or 100)
+        elif c == 2:
+            self.w = config2(grid_n=grid or 2000)
+        elif c == 3:
+            g = grid or 256
+            self.w = config3(grid_n=(g, g, max(1, g // 4)))
+        elif c == 4:
+            self.w = config4(grid_n=grid or 2048)
+        elif c == 5:
+            self.w = config5(grid_n=grid or 512)
+        else:
+            raise ValueError(f"unknown configuration {c}")
+        self.st = bool(self.w.get("st", False))
+        self.blocks = st_blocks(self.w) if self.st else None
+        self.ntarget = len(self.w["grid"])
+        self.nobs = int(sum(len(o["coord"]) for o in self.w["obs"]))
+
+    @property
+    def name(self):
+        return self.w["name"]
+
+    def pq(self):
+        """(drift + unbiasedness rows, variables) of one system."""
+        kw = self.w["kw"]
+        q = self.w["nvar"]
+        aug = q if kw.get("std_ck", False) or self.st else 1
+        return kw.get("ndrift", 0) + aug, q
+
+    def ndim(self):
+        return self.w["ndim"]
+
+    def product(self, precision, nmin=None, idx=None):
+        from krigekit_b200 import Kriging, SpaceTimeKriging
+        nmin = self.w["nmin"] if nmin is None else nmin
+        if self.st:
+            k = SpaceTimeKriging(nvar=1, precision=precision, nmin=nmin)
+        else:
+            k = Kriging(ndim=self.w["ndim"], nvar=self.w["nvar"], precision=precision, nmin=nmin, **self.w["kw"])
+        return self.configure(k, idx)
+
+    def oracle(self, nmin=None, idx=None):
+        from oracle.oracle import OracleKriging, OracleSpaceTime
+        nmin = self.w["nmin"] if nmin is None else nmin
+        if self.st:
+            k = OracleSpaceTime(ndim=2, nmin=nmin)
+        else:
+            k = OracleKriging(ndim=self.w["ndim"], nvar=self.w["nvar"], nmin=nmin, **self.w["kw"])
+        return self.configure(k, idx)
+
+    def configure(self, k, idx=None):
+        """Observations, variograms, targets and search of this workload on k."""
+        w = self.w
+        if self.st:
+            apply_st(k, w, set_grid=False)
+        else:
+            apply(k, w, set_grid=False)
+        self.set_targets(k, idx)
+        return k
+
+    def set_targets(self, k, idx=None):
+        """Targets idx (all by default) on k; returns the host bytes passed."""
+        w = self.w
+        idx = np.arange(self.ntarget) if idx is None else np.asarray(idx)
+        if self.st:
+            b = st_block_subset(self.blocks, idx)
+            set_st_blocks(k, b)
+            return sum(a.nbytes for a in b.values())
+        g = w["grid"][idx]
+        k.set_grid(g)
+        nbytes = g.nbytes
+        if "grid_drift" in w:
+            d = w["grid_drift"][idx]
+            k.set_grid_drift(d)
+            nbytes += d.nbytes
+        return nbytes
+
+    def set_data(self, k, idx=None):
+        """What a caller passes for every solve: observations, targets, search.
+        Variograms stay on k.  Returns the host bytes passed."""
+        w = self.w
+        nbytes = 0
+        for iv, o in enumerate(w["obs"], start=1):
+            k.set_obs(iv, o["coord"], o["value"], nmax=o.get("nmax"), maxdist=o.get("maxdist"))
+            nbytes += o["coord"].nbytes + o["value"].nbytes
+            if "drift" in o:
+                k.set_obs_drift(iv, o["drift"])
+                nbytes += o["drift"].nbytes
+        nbytes += self.set_targets(k, idx)
+        for iv, s in enumerate(w["search"], start=1):
+            k.set_search(iv, **s)
+        return nbytes
+
+    def describe(self):
+        o = self.w["obs"][0]
+        s = self.w["search"][0]
+        parts = [f"nmax {o.get('nmax')}"]
+        if s.get("sector_search"):
+            parts.append(f"{2 ** self.w['ndim']} sectors x {o.get('nmax')}")
+        if self.w["kw"].get("anisotropic_search"):
+            parts.append(f"anisotropic search {s}")
+        if self.st:
+            parts.append(f"time_at {s.get('time_at')}, block support on 1/{self.w['block_every']} of the targets")
+        return ", ".join(parts)
 
 
 def rel_err(x, ref, floor):
