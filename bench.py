@@ -38,11 +38,12 @@ METRIC = "kriged targets/s on 1 B200: FP32+refine batched vs FP64 plain at <=1e-
 
 # DRAM bytes per target of the dominant kernels, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload on its
-# 400 x 400 target grid (160 000 targets), scaled to a launch by the targets
-# it processes; the traffic is the neighbour lists and observation gathers and
-# grows in proportion to the targets.
-NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (52.349e6 + 0.751e6) / 160000,
-                             "search": (8.670e6 + 0.899e6) / 160000}
+# 400 x 400 target grid: the factorisation launch covers one 65 536-target
+# chunk (its traffic is the chunk's K64 read back, 16.6 KB per target), the
+# search launch all 160 000 targets (coordinates and neighbour lists); both
+# grow in proportion to the targets.
+NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (1082.661e6 + 4.988e6) / 65536,
+                             "search": (8.669e6 + 1.457e6) / 160000}
 
 
 def solve_flops(n, p=1, q=1):
@@ -404,7 +405,7 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
                          "frac": achieved / peaks["fp32"],
                          "traffic": NCU_DRAM_BYTES_PER_TARGET["solve_fp32_refine"] * ntarget if ncu_known else None,
-                         "traffic_note": ("ncu DRAM bytes per target (400x400 grid) x targets per launch"
+                         "traffic_note": ("ncu DRAM bytes per target (400x400 grid) x targets of the solve"
                                           if ncu_known else "no ncu capture of this workload"),
                          "kernel": "k_solve_warp<float,32|64,refine> (solve phase, CUDA-core FP32)",
                          "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live",
