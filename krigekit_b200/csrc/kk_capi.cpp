@@ -139,6 +139,7 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
   e->st = 0;
   e->nblock = 0;
   e->bcoord.clear(); e->nblockpnt.clear(); e->gcoord.clear(); e->gweight.clear();
+  e->bcoord_staged = false;
   e->rangescale.clear(); e->localnugget.clear(); e->bdrift.clear();
   e->grid_dirty = true;
   e->solved = false;
@@ -288,6 +289,27 @@ int krige_set_vgm(int64_t h, int ivar, int jvar, const char* vtype, double nugge
   KK_GUARD_END
 }
 
+// Point-target coordinates straight into the handle's pinned staging buffer
+// (one host copy; the solve uploads it as is and splits the axes on the
+// device).  False when pinned memory cannot be had: the caller keeps the
+// coordinates in bcoord instead.
+static bool stage_targets(Engine* e, const double* coord, size_t nval) {
+  const size_t need = sizeof(double) * nval;
+  if (e->hstage_bytes < need) {
+    if (e->hstage) cudaFreeHost(e->hstage);
+    e->hstage = nullptr;
+    e->hstage_bytes = 0;
+    if (cudaHostAlloc(&e->hstage, need, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      e->hstage = nullptr;
+      return false;
+    }
+    e->hstage_bytes = need;
+  }
+  if (need) std::memcpy(e->hstage, coord, need);
+  return true;
+}
+
 static void grid_common(Engine* e, int nblock, const double* rangescale, const double* localnugget) {
   e->nblock = nblock;
   e->rangescale.clear();
@@ -311,7 +333,10 @@ int krige_set_grid(int64_t h, int ngrid, int ndim_c, const double* coord, const 
   if (!e) return 1;
   if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
   if (ndim_c != e->nlag) throw std::string("nlag /= size(coord, 1) for self%grid");
-  e->bcoord.assign(coord, coord + (size_t)ndim_c * ngrid);
+  const size_t nval = (size_t)ndim_c * ngrid;
+  e->bcoord_staged = stage_targets(e, coord, nval);
+  if (e->bcoord_staged) e->bcoord.clear();
+  else e->bcoord.assign(coord, coord + nval);
   e->nblockpnt.clear();
   e->gcoord.clear();
   e->gweight.clear();
@@ -338,6 +363,7 @@ int krige_set_grid_block(int64_t h, int block_type, int ngrid, int ndim_c, const
     int ngq = 1;
     for (int k = 0; k < D; ++k) ngq *= 4;
     e->bcoord.assign(coord, coord + (size_t)D * nb);
+    e->bcoord_staged = false;
     e->nblockpnt.assign(nb, ngq);
     e->gcoord.assign((size_t)D * nb * ngq, 0.0);
     e->gweight.assign((size_t)nb * ngq, 0.0);
@@ -371,6 +397,7 @@ int krige_set_grid_block(int64_t h, int block_type, int ngrid, int ndim_c, const
     }
     // weighted centroid (set_grid_centroid_common, kriging_base.F90:1546-1560)
     e->bcoord.assign((size_t)D * nblock, 0.0);
+    e->bcoord_staged = false;
     size_t g0 = 0;
     for (int ib = 0; ib < nblock; ++ib) {
       const int nn = nblockpnt[ib];
@@ -397,6 +424,7 @@ int krige_set_grid_cv(int64_t h) {
   if (e->obs.empty() || e->obs[0].n == 0) throw std::string("Observation needs to be set first.");
   e->cross_validation = 1;
   e->bcoord = e->obs[0].coord;
+  e->bcoord_staged = false;
   e->nblockpnt.clear();
   e->gcoord.clear();
   e->gweight.clear();
@@ -497,8 +525,12 @@ int krige_get_block_coord(int64_t h, int ndim_c, int nblocks, double* out) {
   KK_GUARD_BEGIN
   Engine* e = get(h);
   if (!e) return 1;
+  const double* bc = e->bcoord_staged ? static_cast<const double*>(e->hstage) : e->bcoord.data();
+  if (!bc || (!e->bcoord_staged && e->bcoord.size() < (size_t)e->nblock * e->nlag))
+    throw std::string("no target coordinates are set");
+  if (ndim_c > e->nlag) throw std::string("ndim exceeds the coordinate dimension of the targets");
   for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib)
-    for (int k = 0; k < ndim_c; ++k) out[(size_t)ib * ndim_c + k] = e->bcoord[(size_t)ib * e->nlag + k];
+    for (int k = 0; k < ndim_c; ++k) out[(size_t)ib * ndim_c + k] = bc[(size_t)ib * e->nlag + k];
   KK_GUARD_END
 }
 
@@ -858,6 +890,7 @@ int krige_st_set_grid_block(int64_t h, int nblocks, const double* coord, const d
   }
   if (tot != npnts_total) throw std::string("sum(nblockpnt) /= size(blockcoord, 2)");
   e->bcoord = st_coords(e, nblocks, coord, time);
+  e->bcoord_staged = false;
   e->nblockpnt.assign(nblockpnt, nblockpnt + nblocks);
   e->gcoord = st_coords(e, npnts_total, blockcoord, blocktime);
   e->gweight.assign(pointweight, pointweight + npnts_total);

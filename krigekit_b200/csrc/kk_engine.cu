@@ -67,6 +67,18 @@ static void upload(DBuf& d, const void* h, size_t bytes, cudaStream_t st) {
   if (bytes) KK_CUDA(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, st));
 }
 
+// (D, nb) interleaved target coordinates -> one array per axis
+__global__ void k_split_axes(const double* __restrict__ src, int nb, int D, double* __restrict__ x0,
+                             double* __restrict__ x1, double* __restrict__ x2, double* __restrict__ x3) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    const double* p = src + (size_t)i * D;
+    x0[i] = p[0];
+    if (D > 1) x1[i] = p[1];
+    if (D > 2) x2[i] = p[2];
+    if (D > 3) x3[i] = p[3];
+  }
+}
+
 static int sm_count(int dev) {
   static int cached[64] = {0};
   if (dev < 0 || dev >= 64) return 148;
@@ -446,7 +458,8 @@ void engine_solve(Engine& e) {
 
   // ---- targets
   if (e.grid_dirty) {
-    // target coordinates: transposed into pinned staging, one copy per axis
+    // target coordinates: through pinned staging, one array per axis on the
+    // device
     const size_t need = sizeof(double) * (size_t)nb * D;
     if (e.hstage_bytes < need) {
       if (e.hstage) cudaFreeHost(e.hstage);
@@ -456,9 +469,23 @@ void engine_solve(Engine& e) {
       e.hstage_bytes = need;
     }
     double* hs = static_cast<double*>(e.hstage);
-    for (int i = 0; i < nb; ++i)
-      for (int k = 0; k < D; ++k) hs[(size_t)k * nb + i] = e.bcoord[(size_t)i * D + k];
-    for (int k = 0; k < D; ++k) upload(e.tx[k], hs + (size_t)k * nb, sizeof(double) * nb, st);
+    if (e.bcoord_staged) {
+      // the caller's (D, nb) layout as staged by krige_set_grid: one copy,
+      // then the per-axis split on the device
+      upload(e.til, hs, need, st);
+      for (int k = 0; k < D; ++k) e.tx[k].reserve(sizeof(double) * nb);
+      if (nb > 0) {
+        k_split_axes<<<std::min((nb + 255) / 256, 8 * nsm), 256, 0, st>>>(
+            e.til.as<double>(), nb, D, e.tx[0].as<double>(), D > 1 ? e.tx[1].as<double>() : nullptr,
+            D > 2 ? e.tx[2].as<double>() : nullptr, D > 3 ? e.tx[3].as<double>() : nullptr);
+        KK_CUDA(cudaGetLastError());
+        e.launches += 1;
+      }
+    } else {
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < D; ++k) hs[(size_t)k * nb + i] = e.bcoord[(size_t)i * D + k];
+      for (int k = 0; k < D; ++k) upload(e.tx[k], hs + (size_t)k * nb, sizeof(double) * nb, st);
+    }
     for (int k = D; k < 4; ++k) e.tx[k].reserve(8);
     if (!e.rangescale.empty()) upload(e.trs, e.rangescale.data(), sizeof(double) * nb, st);
     if (!e.localnugget.empty()) upload(e.tln, e.localnugget.data(), sizeof(double) * nb, st);
@@ -685,7 +712,7 @@ void engine_release(Engine& e) {
   for (auto& b : e.gx) b.release();
   e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
   e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
-  e.counters.release(); e.scratch.release(); e.kbuf.release();
+  e.counters.release(); e.scratch.release(); e.kbuf.release(); e.til.release();
   if (e.hstage) cudaFreeHost(e.hstage);
   e.hstage = nullptr;
   e.hstage_bytes = 0;

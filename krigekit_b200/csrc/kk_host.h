@@ -81,7 +81,8 @@ struct Engine {
 
   // targets
   int nblock = 0;
-  std::vector<double> bcoord;       // (nlag, nblock)
+  std::vector<double> bcoord;       // (nlag, nblock); empty when bcoord_staged
+  bool bcoord_staged = false;       // point targets held in hstage (nlag, nblock) instead
   std::vector<int> nblockpnt;       // empty -> point targets
   std::vector<double> gcoord, gweight;
   std::vector<double> rangescale, localnugget;
@@ -93,6 +94,7 @@ struct Engine {
   DBuf models, tables, tx[4], trs, tln, tdrift, gstart, gx[4], gw;
   DBuf est, var, status, npp, bucket, counters, scratch;
   DBuf kbuf;  // packed K64 of one chunk of targets (assembly -> factorisation)
+  DBuf til;  // point-target coordinates as given (nlag, nblock), before the per-axis split
   void* hstage = nullptr;  // pinned host staging for target uploads
   size_t hstage_bytes = 0;
   size_t scratch_bytes = 0;

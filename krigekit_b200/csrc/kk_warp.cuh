@@ -82,8 +82,11 @@ __device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, cons
 // that the rarely taken shape code does not raise the kernels' register count
 __device__ __noinline__ double tail_cov(const KkModel* m, double h) { return model_cov_h(*m, h); }
 
-// COV(vgm(first, second), lag) for models without the fast path
-__device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, int second, const double* lag) {
+// COV(vgm(first, second), lag) for models without the fast path; the lag
+// travels by value so that callers keep it in registers
+__device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, int second, double l0, double l1,
+                                             double l2, double l3) {
+  const double lag[4] = {l0, l1, l2, l3};
   return cov_pair(P, first, second, lag);
 }
 
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? fast_cov(P, zr, lag) : cov_pair_call(P, vr, s.var[c], lag);
+        kv = fast ? fast_cov(P, zr, lag) : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
       c += 32;
