@@ -312,13 +312,14 @@ __device__ void warp_sort_ints(int* v, int n) {
 }
 
 // Select the K smallest squared distances among candidates [0, M) for which
-// pred(j) holds; appends their (idx, d2) to out[*nout ...].  Returns the K-th
+// pred(j) holds; appends their (idx, d2) to out[*nout ...] when emit is set
+// (out and outd then hold at least *nout + K entries).  Returns the K-th
 // smallest value T in *T_out and sets *tie when a candidate outside the
 // selection has distance exactly T.  Returns false when the boundary bucket
 // overflows the boundary buffer.
 template <class Pred>
-__device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bcap, Pred pred, int* nout,
-                            double* T_out, bool* tie) {
+__device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bcap, Pred pred, bool emit,
+                            int* nout, double* T_out, bool* tie) {
   const int lane = threadIdx.x & 31;
   for (int i = lane; i < NBIN; i += 32) b.hist[i] = 0;
   __syncwarp();
@@ -364,7 +365,7 @@ __device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bc
     }
     unsigned lo = __ballot_sync(0xffffffffu, bin >= 0 && bin < B);
     unsigned eq = __ballot_sync(0xffffffffu, bin == B);
-    if (bin >= 0 && bin < B) {
+    if (emit && bin >= 0 && bin < B) {
       int p = no + __popc(lo & lanemask_lt());
       b.out[p] = b.idx[j];
       b.outd[p] = b.d2[j];
@@ -385,7 +386,8 @@ __device__ bool warp_select(const WarpBuf& b, int M, int K, double dmax2, int bc
   __syncwarp();
   warp_sort_pairs(b.bd2, b.bidx, np2);
   const int r = K - cb;
-  for (int i = lane; i < r; i += 32) { b.out[no + i] = b.bidx[i]; b.outd[no + i] = b.bd2[i]; }
+  if (emit)
+    for (int i = lane; i < r; i += 32) { b.out[no + i] = b.bidx[i]; b.outd[no + i] = b.bd2[i]; }
   double T = b.bd2[r - 1];
   *tie = (r < nb) && (b.bd2[r] == T);
   *T_out = T;
@@ -535,16 +537,30 @@ __device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax
 }
 
 // Per-warp candidate buffers of k_search: CAP candidates {d2, idx, sector},
-// OCAP selected, BCAP boundary-bucket entries and the 256-bin histogram.
-// Sized so that three 4-warp CTAs fit on an SM; a target whose ball holds
-// more than CAP points, or that asks for OCAP or more candidates, takes the
-// exact kd-tree path instead.
+// ocap selected indices (and their distances when ocapd > 0), bcap
+// boundary-bucket entries and the 256-bin histogram.  The plain k-nearest
+// search keeps the K selected with their distances (ocap = ocapd = 320, three
+// 4-warp CTAs per SM).  The sector search only needs the K-th distance of
+// the first selection and keeps the 2^ndim * nmax sector picks, so its
+// buffers are smaller (four CTAs per SM in 2-D).  A target whose ball holds
+// more than CAP points, or whose selection does not fit these buffers, takes
+// the exact kd-tree path instead.
 constexpr int KK_SEARCH_OCAP = 320;
 constexpr int KK_SEARCH_BCAP = 256;
+constexpr int KK_SEARCH_BCAP_SECTOR = 240;
+#ifndef KK_SEARCH_BISECT
+#define KK_SEARCH_BISECT 5  // radius bisection steps
+#endif
+struct SearchLayout {
+  int ocap, ocapd, bcap;
+};
+__host__ __device__ inline SearchLayout search_layout(const KkSearch& S) {
+  if (S.mode == 2) return {((((1 << S.ndim) * S.nmax + 1) + 31) / 32) * 32, 0, KK_SEARCH_BCAP_SECTOR};
+  return {KK_SEARCH_OCAP, KK_SEARCH_OCAP, KK_SEARCH_BCAP};
+}
 template <int CAP>
-__host__ __device__ constexpr size_t search_smem_per_warp() {
-  return sizeof(double) * (CAP + KK_SEARCH_OCAP + KK_SEARCH_BCAP) +
-         sizeof(int) * (CAP + KK_SEARCH_OCAP + KK_SEARCH_BCAP + 256) + CAP;
+__host__ __device__ inline size_t search_smem_per_warp(const SearchLayout& L) {
+  return sizeof(double) * (CAP + L.ocapd + L.bcap) + sizeof(int) * (CAP + L.ocap + L.bcap + 256) + CAP;
 }
 
 template <int CAP>
@@ -556,15 +572,15 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
                                                 int* __restrict__ nnear, int* __restrict__ status,
                                                 int* __restrict__ redo_list, int* __restrict__ redo_count) {
   constexpr int WARPS = 4;
-  constexpr int BCAP = KK_SEARCH_BCAP;
-  constexpr int OCAP = KK_SEARCH_OCAP;
+  const SearchLayout LY = search_layout(S);
+  const int BCAP = LY.bcap, OCAP = LY.ocap;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned char* base = smem_raw + (size_t)w * search_smem_per_warp<CAP>();
+  unsigned char* base = smem_raw + (size_t)w * search_smem_per_warp<CAP>(LY);
   WarpBuf B;
   B.d2 = reinterpret_cast<double*>(base);
-  B.outd = B.d2 + CAP;
-  B.bd2 = B.outd + OCAP;
+  B.outd = B.d2 + CAP;  // LY.ocapd entries (none in the sector layout)
+  B.bd2 = B.outd + LY.ocapd;
   B.idx = reinterpret_cast<int*>(B.bd2 + BCAP);
   B.out = B.idx + CAP;
   B.bidx = B.out + OCAP;
@@ -677,8 +693,17 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
     // cells already hold K + 1 points (the corner ball of the box can reach
     // far into a neighbouring cluster)
     {
-      double rhi = sqrt(D2), rlo = 0.0;
-      for (int it = 0; it < 8; ++it) {
+      // lower bracket: a cell outside the ring-(R-1) box, which holds fewer
+      // than K + 1 points, has its farthest corner at least R cell widths
+      // away, so no smaller ball covers K + 1 points with whole cells (the
+      // bracket only sets how fast the bisection closes: rhi stays a radius
+      // whose covered cells hold K + 1 points)
+      double hmin = g.h[0];
+#pragma unroll
+      for (int k = 1; k < 3; ++k)
+        if (k < g.G) hmin = fmin(hmin, g.h[k]);
+      double rhi = sqrt(D2), rlo = fmin(R * hmin * (1.0 - 1e-6), rhi);
+      for (int it = 0; it < KK_SEARCH_BISECT; ++it) {
         const double mid = 0.5 * (rlo + rhi);
         if (inner_count(g, q, qg, mid * mid, lane) >= (long long)K + 1) rhi = mid;
         else rlo = mid;
@@ -780,14 +805,15 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
       }
     }
     __syncwarp();
-    if (overflow || M < K || K >= OCAP) {
+    if (overflow || M < K || (S.mode != 2 && K >= OCAP)) {
       st |= KK_ST_OVERFLOW;
     } else {
       double T;
       bool tie = false;
       int nout = 0;
       // K nearest (kdtree2_n_nearest semantics: the K smallest distances)
-      bool ok = warp_select(B, M, K, D2, BCAP, [](int) { return true; }, &nout, &T, &tie);
+      // the sector search keeps only the K-th distance T of this selection
+      bool ok = warp_select(B, M, K, D2, BCAP, [](int) { return true; }, S.mode != 2, &nout, &T, &tie);
       if (!ok) st |= KK_ST_OVERFLOW;
       else if (tie && T <= S.maxd2) st |= KK_ST_TIE;
       if (!(st & (KK_ST_OVERFLOW | KK_ST_TIE))) {
@@ -1079,11 +1105,16 @@ void launch_search(const KkSearch& S, int ntarget, const double* const* tx, cons
   int cap_blocks = nsm * 8;
   if (blocks > cap_blocks) blocks = cap_blocks;
   if (blocks < 1) blocks = 1;
-  const size_t smem = 4 * search_smem_per_warp<768>();
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_search<768>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
+  const size_t smem = 4 * search_smem_per_warp<768>(search_layout(S));
+  static bool attr[64] = {false};  // per device: function attributes belong to a context
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr[dev]) {
+    // the largest layout; the sector layout lets more CTAs share an SM
+    cudaFuncSetAttribute(k_search<768>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(4 * search_smem_per_warp<768>(SearchLayout{KK_SEARCH_OCAP, KK_SEARCH_OCAP, KK_SEARCH_BCAP})));
+    cudaFuncSetAttribute(k_search<768>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (dev >= 0 && dev < 64) attr[dev] = true;
   }
   k_search<768><<<blocks, 128, smem, st>>>(S, ntarget, tx[0], tx[1], tx[2], tx[3], ox[0], ox[1], ox[2], ox[3], nbr,
                                         nnear, status, redo_list, redo_count);
