@@ -293,21 +293,37 @@ class Workload:
         self.set_targets(k, idx)
         return k
 
+    def targets(self, idx=None):
+        """Host arrays of the targets idx (all by default), built once per idx:
+        a caller holds its targets already, so building them is not part of a
+        solve."""
+        key = None if idx is None else (len(idx), int(idx[0]) if len(idx) else 0, int(idx[-1]) if len(idx) else 0)
+        cache = self.__dict__.setdefault("_tcache", {})
+        if key in cache:
+            return cache[key]
+        w = self.w
+        sel = np.arange(self.ntarget) if idx is None else np.asarray(idx)
+        if self.st:
+            t = dict(blocks=st_block_subset(self.blocks, sel))
+        else:
+            t = dict(grid=np.ascontiguousarray(w["grid"][sel]))
+            if "grid_drift" in w:
+                t["grid_drift"] = np.ascontiguousarray(w["grid_drift"][sel])
+        cache.clear()
+        cache[key] = t
+        return t
+
     def set_targets(self, k, idx=None):
         """Targets idx (all by default) on k; returns the host bytes passed."""
-        w = self.w
-        idx = np.arange(self.ntarget) if idx is None else np.asarray(idx)
+        t = self.targets(idx)
         if self.st:
-            b = st_block_subset(self.blocks, idx)
-            set_st_blocks(k, b)
-            return sum(a.nbytes for a in b.values())
-        g = w["grid"][idx]
-        k.set_grid(g)
-        nbytes = g.nbytes
-        if "grid_drift" in w:
-            d = w["grid_drift"][idx]
-            k.set_grid_drift(d)
-            nbytes += d.nbytes
+            set_st_blocks(k, t["blocks"])
+            return sum(a.nbytes for a in t["blocks"].values())
+        k.set_grid(t["grid"])
+        nbytes = t["grid"].nbytes
+        if "grid_drift" in t:
+            k.set_grid_drift(t["grid_drift"])
+            nbytes += t["grid_drift"].nbytes
         return nbytes
 
     def set_data(self, k, idx=None):

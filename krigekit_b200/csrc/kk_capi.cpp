@@ -846,14 +846,14 @@ int krige_st_set_vgm_joint_sills(int64_t h, int ivar, int jvar, int nsill, const
 }
 
 // spatial coordinates (ndim, n) and times (n) -> (ndim + 1, n)
-static std::vector<double> st_coords(const Engine* e, int n, const double* coord, const double* time) {
+// coord(nd, n) + time(n) -> c(nd + 1, n); c keeps its capacity across calls
+static void st_coords(const Engine* e, int n, const double* coord, const double* time, std::vector<double>& c) {
   const int nd = e->ndim;
-  std::vector<double> c((size_t)(nd + 1) * n);
+  c.resize((size_t)(nd + 1) * n);
   for (int i = 0; i < n; ++i) {
     for (int k = 0; k < nd; ++k) c[(size_t)i * (nd + 1) + k] = coord[(size_t)i * nd + k];
     c[(size_t)i * (nd + 1) + nd] = time[i];
   }
-  return c;
 }
 
 // krige_st_set_grid, kriging_st_capi.f90:331-353: coord(ndim, ngrid), time(ngrid)
@@ -864,7 +864,7 @@ int krige_st_set_grid(int64_t h, int ngrid, const double* coord, const double* t
     KK_GUARD_BEGIN
     Engine* e = get_st(h);
     if (!e) return 1;
-    c = st_coords(e, ngrid, coord, time);
+    st_coords(e, ngrid, coord, time, c);
     KK_GUARD_END_NORET
   }
   if (failed()) return 1;
@@ -889,10 +889,10 @@ int krige_st_set_grid_block(int64_t h, int nblocks, const double* coord, const d
     tot += nblockpnt[i];
   }
   if (tot != npnts_total) throw std::string("sum(nblockpnt) /= size(blockcoord, 2)");
-  e->bcoord = st_coords(e, nblocks, coord, time);
+  st_coords(e, nblocks, coord, time, e->bcoord);
   e->bcoord_staged = false;
   e->nblockpnt.assign(nblockpnt, nblockpnt + nblocks);
-  e->gcoord = st_coords(e, npnts_total, blockcoord, blocktime);
+  st_coords(e, npnts_total, blockcoord, blocktime, e->gcoord);
   e->gweight.assign(pointweight, pointweight + npnts_total);
   grid_common(e, nblocks, rangescale, localnugget);
   KK_GUARD_END

@@ -459,9 +459,20 @@ void engine_solve(Engine& e) {
   // ---- targets
   if (e.grid_dirty) {
     // target coordinates: through pinned staging, one array per axis on the
-    // device
-    const size_t need = sizeof(double) * (size_t)nb * D;
+    // device; block targets add their nodes, weights and node offsets after
+    // them in the same staging buffer (every region is in flight until the
+    // synchronisation below)
+    const bool blocks = !e.nblockpnt.empty();
+    size_t ng = 0;
+    if (blocks)
+      for (int i = 0; i < nb; ++i) ng += (size_t)e.nblockpnt[i];
+    const size_t need_t = sizeof(double) * (size_t)nb * D;
+    const size_t need_n = blocks ? sizeof(double) * ng * (D + 1) : 0;
+    const size_t need_g = blocks ? sizeof(int) * ((size_t)nb + 1) : 0;
+    const size_t need = need_t + need_n + need_g;
     if (e.hstage_bytes < need) {
+      // never reached with staged point targets: krige_set_grid sized the
+      // buffer for them and they carry no nodes
       if (e.hstage) cudaFreeHost(e.hstage);
       e.hstage = nullptr;
       e.hstage_bytes = 0;
@@ -472,7 +483,7 @@ void engine_solve(Engine& e) {
     if (e.bcoord_staged) {
       // the caller's (D, nb) layout as staged by krige_set_grid: one copy,
       // then the per-axis split on the device
-      upload(e.til, hs, need, st);
+      upload(e.til, hs, need_t, st);
       for (int k = 0; k < D; ++k) e.tx[k].reserve(sizeof(double) * nb);
       if (nb > 0) {
         k_split_axes<<<std::min((nb + 255) / 256, 8 * nsm), 256, 0, st>>>(
@@ -489,17 +500,17 @@ void engine_solve(Engine& e) {
     for (int k = D; k < 4; ++k) e.tx[k].reserve(8);
     if (!e.rangescale.empty()) upload(e.trs, e.rangescale.data(), sizeof(double) * nb, st);
     if (!e.localnugget.empty()) upload(e.tln, e.localnugget.data(), sizeof(double) * nb, st);
-    if (!e.nblockpnt.empty()) {
-      std::vector<int> gs(nb + 1, 0);
+    if (blocks) {
+      double* hn = hs + (size_t)nb * D;  // nodes per axis, then the weights
+      for (size_t i = 0; i < ng; ++i)
+        for (int k = 0; k < D; ++k) hn[(size_t)k * ng + i] = e.gcoord[i * D + k];
+      std::memcpy(hn + (size_t)D * ng, e.gweight.data(), sizeof(double) * ng);
+      int* gs = reinterpret_cast<int*>(hn + (size_t)(D + 1) * ng);
+      gs[0] = 0;
       for (int i = 0; i < nb; ++i) gs[i + 1] = gs[i] + e.nblockpnt[i];
-      upload(e.gstart, gs.data(), sizeof(int) * gs.size(), st);
-      const int ng = gs[nb];
-      std::vector<double> gt(ng);
-      for (int k = 0; k < D; ++k) {
-        for (int i = 0; i < ng; ++i) gt[i] = e.gcoord[(size_t)i * D + k];
-        upload(e.gx[k], gt.data(), sizeof(double) * ng, st);
-      }
-      upload(e.gw, e.gweight.data(), sizeof(double) * ng, st);
+      upload(e.gstart, gs, sizeof(int) * ((size_t)nb + 1), st);
+      for (int k = 0; k < D; ++k) upload(e.gx[k], hn + (size_t)k * ng, sizeof(double) * ng, st);
+      upload(e.gw, hn + (size_t)D * ng, sizeof(double) * ng, st);
     }
     KK_CUDA(cudaStreamSynchronize(st));
     e.grid_dirty = false;

@@ -197,10 +197,11 @@ class SpaceTimeKriging:
         spatial, t = _split_coords(coord, time)
         coord_f = np.asfortranarray(spatial.T)
         ngrid = coord_f.shape[1]
-        rs_f = _farray(rangescale if rangescale is not None else np.ones(ngrid))
-        ln_f = _farray(localnugget if localnugget is not None else np.zeros(ngrid))
-        _lib.call("krige_st_set_grid", self._h(), ngrid, _dptr(coord_f), _dptr(_farray(t)), _dptr(rs_f),
-                  _dptr(ln_f))
+        # absent rangescale / localnugget: null (all ones / zeros in the library)
+        rs_f = _farray(rangescale) if rangescale is not None else None
+        ln_f = _farray(localnugget) if localnugget is not None else None
+        _lib.call("krige_st_set_grid", self._h(), ngrid, _dptr(coord_f), _dptr(_farray(t)),
+                  None if rs_f is None else _dptr(rs_f), None if ln_f is None else _dptr(ln_f))
 
     def set_grid_block(self, coord, time, nblockpnt, block_coord, block_time, pointweight=None,
                        rangescale=None, localnugget=None):
@@ -218,11 +219,13 @@ class SpaceTimeKriging:
         npnt = g.shape[1]
         if pointweight is None:
             pointweight = np.repeat(1.0 / nbp, nbp)
-        rs_f = _farray(rangescale if rangescale is not None else np.ones(nb))
-        ln_f = _farray(localnugget if localnugget is not None else np.zeros(nb))
+        # absent rangescale / localnugget: null (all ones / zeros in the library)
+        rs_f = _farray(rangescale) if rangescale is not None else None
+        ln_f = _farray(localnugget) if localnugget is not None else None
         _lib.call("krige_st_set_grid_block", self._h(), nb, _dptr(c), _dptr(_farray(np.ravel(time))),
                   _iptr(nbp), npnt, _dptr(g), _dptr(_farray(np.ravel(block_time))),
-                  _dptr(_farray(np.ravel(pointweight))), _dptr(rs_f), _dptr(ln_f))
+                  _dptr(_farray(np.ravel(pointweight))), None if rs_f is None else _dptr(rs_f),
+                  None if ln_f is None else _dptr(ln_f))
 
     def set_grid_cv(self):
         """Cross-validation targets at the observations."""
