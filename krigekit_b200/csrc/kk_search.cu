@@ -539,28 +539,46 @@ __device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax
 // Per-warp candidate buffers of k_search: CAP candidates {d2, idx, sector},
 // ocap selected indices (and their distances when ocapd > 0), bcap
 // boundary-bucket entries and the 256-bin histogram.  The plain k-nearest
-// search keeps the K selected with their distances (ocap = ocapd = 320, three
-// 4-warp CTAs per SM).  The sector search only needs the K-th distance of
-// the first selection and keeps the 2^ndim * nmax sector picks, so its
-// buffers are smaller (four CTAs per SM in 2-D).  A target whose ball holds
-// more than CAP points, or whose selection does not fit these buffers, takes
-// the exact kd-tree path instead.
+// search keeps the K selected with their distances (ocap = ocapd, the next
+// multiple of 32 above K, at most 320).  The sector search only needs the
+// K-th distance of the first selection and keeps the 2^ndim * nmax sector
+// picks (ocapd = 0).  The boundary buffer takes what is left of a quarter of
+// the SM's shared memory, so that four 4-warp CTAs share an SM, when that
+// leaves at least 128 entries; otherwise it holds 256 and three CTAs fit.  A
+// target whose ball holds more than CAP points, or whose selection does not
+// fit these buffers, takes the exact kd-tree path instead.
 constexpr int KK_SEARCH_OCAP = 320;
 constexpr int KK_SEARCH_BCAP = 256;
-constexpr int KK_SEARCH_BCAP_SECTOR = 240;
+constexpr int KK_SMEM_PER_SM = 233472;  // 228 KB of shared memory per SM
+constexpr int KK_SMEM_PER_CTA_RESERVED = 1024;
 #ifndef KK_SEARCH_BISECT
 #define KK_SEARCH_BISECT 5  // radius bisection steps
 #endif
 struct SearchLayout {
   int ocap, ocapd, bcap;
 };
-__host__ __device__ inline SearchLayout search_layout(const KkSearch& S) {
-  if (S.mode == 2) return {((((1 << S.ndim) * S.nmax + 1) + 31) / 32) * 32, 0, KK_SEARCH_BCAP_SECTOR};
-  return {KK_SEARCH_OCAP, KK_SEARCH_OCAP, KK_SEARCH_BCAP};
-}
 template <int CAP>
 __host__ __device__ inline size_t search_smem_per_warp(const SearchLayout& L) {
   return sizeof(double) * (CAP + L.ocapd + L.bcap) + sizeof(int) * (CAP + L.ocap + L.bcap + 256) + CAP;
+}
+template <int CAP>
+__host__ __device__ inline SearchLayout search_layout(const KkSearch& S) {
+  SearchLayout L;
+  if (S.mode == 2) {
+    L.ocap = (((1 << S.ndim) * S.nmax + 1 + 31) / 32) * 32;
+    L.ocapd = 0;
+  } else {
+    L.ocap = (S.K + 1 + 31) / 32 * 32;
+    if (L.ocap > KK_SEARCH_OCAP) L.ocap = KK_SEARCH_OCAP;
+    L.ocapd = L.ocap;
+  }
+  L.bcap = 0;
+  const long long per_warp = (KK_SMEM_PER_SM / 4 - KK_SMEM_PER_CTA_RESERVED) / 4;
+  const long long room = per_warp - (long long)search_smem_per_warp<CAP>(L);
+  long long bcap = room / (long long)(sizeof(double) + sizeof(int));
+  bcap = bcap / 16 * 16;
+  L.bcap = (bcap >= 128) ? (int)(bcap < KK_SEARCH_BCAP ? bcap : KK_SEARCH_BCAP) : KK_SEARCH_BCAP;
+  return L;
 }
 
 template <int CAP>
@@ -572,7 +590,7 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
                                                 int* __restrict__ nnear, int* __restrict__ status,
                                                 int* __restrict__ redo_list, int* __restrict__ redo_count) {
   constexpr int WARPS = 4;
-  const SearchLayout LY = search_layout(S);
+  const SearchLayout LY = search_layout<CAP>(S);
   const int BCAP = LY.bcap, OCAP = LY.ocap;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1105,12 +1123,12 @@ void launch_search(const KkSearch& S, int ntarget, const double* const* tx, cons
   int cap_blocks = nsm * 8;
   if (blocks > cap_blocks) blocks = cap_blocks;
   if (blocks < 1) blocks = 1;
-  const size_t smem = 4 * search_smem_per_warp<768>(search_layout(S));
+  const size_t smem = 4 * search_smem_per_warp<768>(search_layout<768>(S));
   static bool attr[64] = {false};  // per device: function attributes belong to a context
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || !attr[dev]) {
-    // the largest layout; the sector layout lets more CTAs share an SM
+    // the largest layout; smaller ones let more CTAs share an SM
     cudaFuncSetAttribute(k_search<768>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(4 * search_smem_per_warp<768>(SearchLayout{KK_SEARCH_OCAP, KK_SEARCH_OCAP, KK_SEARCH_BCAP})));
     cudaFuncSetAttribute(k_search<768>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);

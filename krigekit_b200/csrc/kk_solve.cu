@@ -1034,10 +1034,13 @@ static void launch_warp(const SolveParams& P, const int* list, const int* cnt, i
                         const double* Kg, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
   const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
-  static bool attr_set = false;  // per instantiation
-  if (!attr_set) {
+  // per instantiation and device: function attributes belong to a context
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
     cudaFuncSetAttribute(k_solve_warp<T, N, REFINE, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE, CB>, 32 * WPC, smem);
