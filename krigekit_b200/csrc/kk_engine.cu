@@ -569,12 +569,26 @@ void engine_solve(Engine& e) {
   // ---- solve parameters
   SolveParams P;
   fill_params(e, P);
-  P.fast_model = (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_B) ? 1 : 0;
+  // fast covariance path: every vgm(i, j) a Level-B table under one common
+  // anisotropy transform (true of one variable, and of a linear model of
+  // coregionalisation whose structures share their anisotropy)
+  P.fast_model = 0;
+  if (!e.st) {
+    bool ok = true;
+    for (int q = 0; q < nv * nv && ok; ++q) {
+      ok = mdl[q].mode == KK_LEVEL_B && mdl[q].ndim == mdl[0].ndim;
+      for (int k = 0; k < 9 && ok; ++k) ok = mdl[q].bmat[k] == mdl[0].bmat[k];
+    }
+    P.fast_model = ok ? 1 : 0;
+  }
   if (P.fast_model) {
     for (int k = 0; k < 9; ++k) P.fm[k] = mdl[0].bmat[k];
     P.fm_ndim = mdl[0].ndim;
-    P.fm_tail = mdl[0].btail;
-    P.fm_tab_off = mdl[0].btab_off;
+    P.fm_tailmask = 0;
+    for (int q = 0; q < nv * nv; ++q) {
+      P.fm_tab_off[q] = mdl[q].btab_off;
+      if (mdl[q].btail) P.fm_tailmask |= 1 << q;
+    }
   }
 
   // ---- bucket by neighbour count

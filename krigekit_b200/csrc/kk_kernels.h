@@ -49,9 +49,11 @@ struct SolveParams {
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
   double refine_tol_corr;    // bound on the FP32 correction term relative to its value
-  int fast_model;            // one variable, spatial, one Level-B table: fast covariance path
-  int fm_ndim, fm_tail, fm_tab_off;  // that model's dimension, analytic tail, table offset
-  double fm[9];              // and its anisotropy transform (bmat)
+  int fast_model;            // spatial, every vgm(i, j) one Level-B table with one common
+                             // anisotropy transform: fast covariance path
+  int fm_ndim, fm_tailmask;  // that transform's dimension; bit i * nvar + j: vgm(i, j) has an analytic tail
+  int fm_tab_off[KK_MAXVAR * KK_MAXVAR];  // table offset of vgm(i, j) at i * nvar + j
+  double fm[9];              // the common anisotropy transform (bmat)
 };
 
 enum {

@@ -110,14 +110,15 @@ __device__ __forceinline__ double aniso_h_fast(const double* m, int ndim, const 
   return h2 > 0.0 ? h2 * rsqrt(h2) : 0.0;
 }
 
-// The single Level-B model of single-variable spatial kriging (P.fast_model):
-// COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past the table.
-// Its transform and table offset travel in the kernel parameters, which the
-// kernels read as uniform constant operands instead of holding registers.
-__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag) {
+// Level-B models under one common anisotropy transform (P.fast_model):
+// COV(vgm(i, j), lag) = table_ij(aniso_h(bmat, lag)), analytic tail past the
+// table; pair = i * nvar + j.  The transform and table offsets travel in the
+// kernel parameters, which the kernels read as constant operands instead of
+// holding registers.
+__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag, int pair) {
   const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
-  if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off, z, h);
-  return P.fm_tail ? tail_cov(P.models, h) : 0.0;
+  if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off[pair], z, h);
+  return ((P.fm_tailmask >> pair) & 1) ? tail_cov(P.models + pair, h) : 0.0;
 }
 
 template <typename T, int N, bool REFINE>
@@ -289,7 +290,8 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? fast_cov(P, zr, lag) : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
+        kv = fast ? fast_cov(P, zr, lag, vr * P.nvar + s.var[c])
+                  : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
       c += 32;
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
 #pragma unroll
                 for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
               }
-              v = dadd(0.0, dmul(fast_cov(P, zr, lag), 1.0));
+              v = dadd(0.0, dmul(fast_cov(P, zr, lag, vr * P.nvar + iv), 1.0));
             } else {
               v = rhs_cov_row(P, t, xr, vr, iv, rs);
             }

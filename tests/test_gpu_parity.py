@@ -163,6 +163,22 @@ def test_config4_small_cokriging(precision):
     _check_values(g, o, w, TOL[precision])
 
 
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_cokriging_shared_anisotropy(precision):
+    """Linear model of coregionalisation whose structures share one range and
+    anisotropy: every vgm(i, j) is one Level-B table under a common transform,
+    which takes the kernels' tabulated covariance path with per-pair tables."""
+    w = bw.config4(grid_n=30, nobs=(2_000, 20_000))
+    vgm = []
+    for (i, j), (bn, be) in {(1, 1): (0.05, 0.95), (1, 2): (0.0, 0.665), (2, 2): (0.05, 0.95)}.items():
+        vgm.append((i, j, dict(vtype="nug", nugget=bn, sill=0.0, a_major=1.0)))
+        vgm.append((i, j, dict(vtype="exp", nugget=0.0, sill=be, a_major=0.3, a_minor1=0.15, azimuth=40.0)))
+    w["vgm"] = vgm
+    g, o = _run_pair(w, precision, nmin=4)
+    _check_neighbours(g, o, nvar=2)
+    _check_values(g, o, w, TOL[precision])
+
+
 def test_ties_use_exact_kdtree_order():
     # obs on an integer lattice, targets at lattice-symmetric points: many equal
     # distances at the selection boundary exercise the exact kd-tree replica
