@@ -569,25 +569,41 @@ void engine_solve(Engine& e) {
   // ---- solve parameters
   SolveParams P;
   fill_params(e, P);
-  // fast covariance path: every vgm(i, j) a Level-B table under one common
-  // anisotropy transform (true of one variable, and of a linear model of
-  // coregionalisation whose structures share their anisotropy)
+  // fast covariance paths of single-variable spatial kriging (with several
+  // variables vgm(i, j), i > j, has no table and is evaluated analytically,
+  // as in the reference: the general path)
   P.fast_model = 0;
-  if (!e.st) {
-    bool ok = true;
-    for (int q = 0; q < nv * nv && ok; ++q) {
-      ok = mdl[q].mode == KK_LEVEL_B && mdl[q].ndim == mdl[0].ndim;
-      for (int k = 0; k < 9 && ok; ++k) ok = mdl[q].bmat[k] == mdl[0].bmat[k];
-    }
-    P.fast_model = ok ? 1 : 0;
-  }
-  if (P.fast_model) {
+  if (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_B) {
+    P.fast_model = 1;
     for (int k = 0; k < 9; ++k) P.fm[k] = mdl[0].bmat[k];
     P.fm_ndim = mdl[0].ndim;
-    P.fm_tailmask = 0;
-    for (int q = 0; q < nv * nv; ++q) {
-      P.fm_tab_off[q] = mdl[q].btab_off;
-      if (mdl[q].btail) P.fm_tailmask |= 1 << q;
+    P.fm_tail = mdl[0].btail;
+    P.fm_tab_off = mdl[0].btab_off;
+  } else if (!e.st && nv == 1 && mdl[0].mode == KK_LEVEL_A && mdl[0].nstruct >= 1 &&
+             mdl[0].nstruct <= KK_FA_MAXS) {
+    // Level A with every structure's transform a multiple k of one matrix
+    // (structures that differ only in range): h_s = k_s * |B lag|
+    const KkModel& m = mdl[0];
+    const KkComp& c0 = m.comp[0];
+    int big = 0;
+    for (int q = 1; q < 9; ++q)
+      if (std::fabs(c0.mat[q]) > std::fabs(c0.mat[big])) big = q;
+    bool ok = c0.mat[big] != 0.0;
+    P.fa_nst = m.nstruct;
+    P.fa_tailmask = 0;
+    for (int s = 0; s < m.nstruct && ok; ++s) {
+      const KkComp& c = m.comp[s];
+      const double k = c.mat[big] / c0.mat[big];
+      ok = !c.is_product && c.tab_off >= 0 && k > 0.0;
+      for (int r = 0; r < 9 && ok; ++r) ok = std::fabs(c.mat[r] - k * c0.mat[r]) <= 1e-12 * std::fabs(c.mat[big]);
+      P.fa_off[s] = c.tab_off;
+      P.fa_k[s] = k;
+      if (c.tail) P.fa_tailmask |= 1 << s;
+    }
+    if (ok) {
+      P.fast_model = 2;
+      for (int k = 0; k < 9; ++k) P.fm[k] = c0.mat[k];
+      P.fm_ndim = m.ndim;
     }
   }
 

@@ -7,6 +7,8 @@
 namespace kk {
 
 // Everything the solve kernels read for one solve() call.
+#define KK_FA_MAXS 4  // structures per vgm(i, j) on the Level-A fast path
+
 struct SolveParams {
   int nvar, ndim, nlag, st;
   int ndrift, pa, naug, std_ck, unbias;
@@ -49,11 +51,14 @@ struct SolveParams {
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
   double refine_tol_corr;    // bound on the FP32 correction term relative to its value
-  int fast_model;            // spatial, every vgm(i, j) one Level-B table with one common
-                             // anisotropy transform: fast covariance path
-  int fm_ndim, fm_tailmask;  // that transform's dimension; bit i * nvar + j: vgm(i, j) has an analytic tail
-  int fm_tab_off[KK_MAXVAR * KK_MAXVAR];  // table offset of vgm(i, j) at i * nvar + j
-  double fm[9];              // the common anisotropy transform (bmat)
+  int fast_model;            // fast covariance path of single-variable spatial kriging:
+                             // 1 = one Level-B table; 2 = Level-A tables of structures
+                             // whose transforms are multiples k * fm of one matrix
+  int fm_ndim, fm_tail, fm_tab_off;  // transform dimension; Level B: analytic tail, table offset
+  double fm[9];              // the anisotropy transform (bmat, or the Level-A common matrix)
+  int fa_nst, fa_tailmask;   // Level A: structures, bit s = structure s has an analytic tail
+  int fa_off[KK_FA_MAXS];    // their table offsets
+  double fa_k[KK_FA_MAXS];   // and transform multiples
 };
 
 enum {

@@ -1061,8 +1061,15 @@ void launch_assemble(const SolveParams& P, int N, const int* list, const int* cn
   int blocks = nsm * 3;  // the launch bound's residency
   const int need = (nitems + 7) / 8;
   if (need < blocks) blocks = need > 0 ? need : 1;
-  if (N == 32) k_assemble<32><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
-  else k_assemble<64><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+  // the fast covariance variant is a template parameter (the general path
+  // runs in the first instantiation with P.fast_model == 0)
+  if (N == 32) {
+    if (P.fast_model == 2) k_assemble<32, 2><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else k_assemble<32, 1><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+  } else {
+    if (P.fast_model == 2) k_assemble<64, 2><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else k_assemble<64, 1><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+  }
 }
 
 void launch_factor(const SolveParams& P, int refine, int N, const int* list, const int* cnt, int item0, int nitems,

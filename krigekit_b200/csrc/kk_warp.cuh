@@ -110,15 +110,33 @@ __device__ __forceinline__ double aniso_h_fast(const double* m, int ndim, const 
   return h2 > 0.0 ? h2 * rsqrt(h2) : 0.0;
 }
 
-// Level-B models under one common anisotropy transform (P.fast_model):
-// COV(vgm(i, j), lag) = table_ij(aniso_h(bmat, lag)), analytic tail past the
-// table; pair = i * nvar + j.  The transform and table offsets travel in the
-// kernel parameters, which the kernels read as constant operands instead of
-// holding registers.
-__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag, int pair) {
+// The single model of single-variable spatial kriging (P.fast_model); its
+// transform and table offsets travel in the kernel parameters, which the
+// kernels read as constant operands instead of holding registers.
+// Level B (1): COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past
+// the table.
+// Level A (2): COV(vgm, lag) = sum over the structures s of
+// table_s(k_s * |fm lag|), in structure order like the general model_cov.
+__device__ __noinline__ double tail_comp(const KkComp* c, double h) { return comp_cov_h(*c, h); }
+template <int FM>  // 1 or 2 when known at compile time, 0: read P.fast_model
+__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag) {
   const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
-  if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off[pair], z, h);
-  return ((P.fm_tailmask >> pair) & 1) ? tail_cov(P.models + pair, h) : 0.0;
+  if (FM == 1 || (FM == 0 && P.fast_model == 1)) {
+    if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off, z, h);
+    return P.fm_tail ? tail_cov(P.models, h) : 0.0;
+  }
+  double res = 0.0;
+#pragma unroll
+  for (int s = 0; s < KK_FA_MAXS; ++s) {
+    if (s < P.fa_nst) {
+      const double hs = P.fa_k[s] * h;
+      double g;
+      if (hs < z.zb3) g = tab_fast(P.tables + P.fa_off[s], z, hs);
+      else g = ((P.fa_tailmask >> s) & 1) ? tail_comp(&P.models[0].comp[s], hs) : 0.0;
+      res = dadd(res, g);
+    }
+  }
+  return res;
 }
 
 template <typename T, int N, bool REFINE>
@@ -247,7 +265,7 @@ __device__ __forceinline__ int gather_rows(const SolveParams& P, int t, int lane
 // This is the part of the solve that is bound by covariance-table latency,
 // so it runs as its own kernel with many resident warps; the factorisation
 // kernel then reads K from this buffer (L2-resident in chunks).
-template <int N>
+template <int N, int FM>
 __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ SolveParams P,
                                                      const int* __restrict__ list,
                                                      const int* __restrict__ list_count, int item0, int nitems,
@@ -290,7 +308,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? fast_cov(P, zr, lag, vr * P.nvar + s.var[c])
+        kv = fast ? fast_cov<FM>(P, zr, lag)
                   : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
@@ -390,7 +408,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
 #pragma unroll
                 for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
               }
-              v = dadd(0.0, dmul(fast_cov(P, zr, lag, vr * P.nvar + iv), 1.0));
+              v = dadd(0.0, dmul(fast_cov<0>(P, zr, lag), 1.0));
             } else {
               v = rhs_cov_row(P, t, xr, vr, iv, rs);
             }

@@ -166,8 +166,8 @@ def test_config4_small_cokriging(precision):
 @pytest.mark.parametrize("precision", PRECISIONS)
 def test_cokriging_shared_anisotropy(precision):
     """Linear model of coregionalisation whose structures share one range and
-    anisotropy: every vgm(i, j) is one Level-B table under a common transform,
-    which takes the kernels' tabulated covariance path with per-pair tables."""
+    anisotropy (Level-B tables for vgm(i, j), i <= j; the reference evaluates
+    the other orientation analytically, and so does this library)."""
     w = bw.config4(grid_n=30, nobs=(2_000, 20_000))
     vgm = []
     for (i, j), (bn, be) in {(1, 1): (0.05, 0.95), (1, 2): (0.0, 0.665), (2, 2): (0.05, 0.95)}.items():
@@ -176,6 +176,19 @@ def test_cokriging_shared_anisotropy(precision):
     w["vgm"] = vgm
     g, o = _run_pair(w, precision, nmin=4)
     _check_neighbours(g, o, nvar=2)
+    _check_values(g, o, w, TOL[precision])
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_nested_ranges_one_variable(precision):
+    """Nested structures that differ only in range (Level-A tables whose
+    transforms are multiples of one matrix), anisotropic, one variable."""
+    w = bw.config1(grid_n=24, nobs=3000)
+    w["vgm"] = [(1, 1, dict(vtype="sph", nugget=0.03, sill=0.6, a_major=0.12, a_minor1=0.06, azimuth=25.0)),
+                (1, 1, dict(vtype="exp", nugget=0.0, sill=0.4, a_major=0.5, a_minor1=0.25, azimuth=25.0))]
+    w["sill"] = 1.03
+    g, o = _run_pair(w, precision, nmin=4)
+    _check_neighbours(g, o)
     _check_values(g, o, w, TOL[precision])
 
 
