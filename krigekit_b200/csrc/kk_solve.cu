@@ -92,22 +92,35 @@ __device__ __forceinline__ void write_nan(const SolveParams& P, int t) {
 // ---------------------------------------------------------------------------
 __global__ void k_bucket(SolveParams P, int* __restrict__ lists) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.nblock) return;
-  int npp = 0;
-  for (int v = 0; v < P.nvar; ++v) npp += P.nnear[v][t];
-  int slot;
-  if (npp == 0 || npp == 1 || (P.nmin > 0 && npp < P.nmin)) {
-    // zero neighbours (kriging_base.F90:3198-3207); npp == 1 reuses a stale
-    // solution in the reference and is reported as NaN here
-    write_nan(P, t);
-    P.status[t] |= KK_ST_EMPTY;
-    if (npp == 0 && !P.neglect_error) atomicAdd(&P.counters[KK_CNT_FAIL], 1);
-    return;
+  const int lane = threadIdx.x & 31;
+  int slot = -1;  // no list: past the targets, or no system to solve
+  if (t < P.nblock) {
+    int npp = 0;
+    for (int v = 0; v < P.nvar; ++v) npp += P.nnear[v][t];
+    if (npp == 0 || npp == 1 || (P.nmin > 0 && npp < P.nmin)) {
+      // zero neighbours (kriging_base.F90:3198-3207); npp == 1 reuses a stale
+      // solution in the reference and is reported as NaN here
+      write_nan(P, t);
+      P.status[t] |= KK_ST_EMPTY;
+      if (npp == 0 && !P.neglect_error) atomicAdd(&P.counters[KK_CNT_FAIL], 1);
+    } else {
+      slot = npp <= 32 ? KK_CNT_B16 : (npp <= 64 ? KK_CNT_B64 : KK_CNT_BIG);
+      if (slot == KK_CNT_BIG) P.status[t] |= KK_ST_BIG;
+    }
   }
-  slot = npp <= 32 ? KK_CNT_B16 : (npp <= 64 ? KK_CNT_B64 : KK_CNT_BIG);
-  if (slot == KK_CNT_BIG) P.status[t] |= KK_ST_BIG;
-  int p = atomicAdd(&P.counters[slot], 1);
-  lists[(size_t)slot * P.nblock + p] = t;
+  // one atomic per warp and list (the order within a list is free: every
+  // target is solved on its own)
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int sl = KK_CNT_B16; sl <= KK_CNT_BIG; ++sl) {
+    const unsigned m = __ballot_sync(0xffffffffu, slot == sl);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&P.counters[sl], __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (slot == sl) lists[(size_t)sl * P.nblock + base + __popc(m & lt)] = t;
+  }
 }
 
 void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st) {
