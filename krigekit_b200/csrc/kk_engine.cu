@@ -605,6 +605,54 @@ void engine_solve(Engine& e) {
       for (int k = 0; k < 9; ++k) P.fm[k] = c0.mat[k];
       P.fm_ndim = m.ndim;
     }
+  } else if (!e.st && nv == 2) {
+    // two variables whose structures all have transforms k * B (structures
+    // that differ only in range and sill, as in a linear model of
+    // coregionalisation): per pair a Level-B table, Level-A tables, or (for
+    // vgm(i, j), i > j) the analytic structures, each at h_s = k_s * |B lag|
+    const KkComp& c0 = mdl[0].comp[0];
+    int big = 0;
+    for (int q = 1; q < 9; ++q)
+      if (std::fabs(c0.mat[q]) > std::fabs(c0.mat[big])) big = q;
+    bool ok = c0.mat[big] != 0.0;
+    auto mult = [&](const double* mat, double& k) {
+      k = mat[big] / c0.mat[big];
+      bool good = k > 0.0;
+      for (int r = 0; r < 9 && good; ++r) good = std::fabs(mat[r] - k * c0.mat[r]) <= 1e-12 * std::fabs(mat[big]);
+      return good;
+    };
+    for (int q = 0; q < 4 && ok; ++q) {
+      const KkModel& m = mdl[q];
+      ok = m.ndim == mdl[0].ndim && m.nstruct >= 1 && m.nstruct <= KK_FA_MAXS;
+      for (int s = 0; s < m.nstruct && ok; ++s) {
+        double k;
+        ok = !m.comp[s].is_product && mult(m.comp[s].mat, k);
+      }
+      if (!ok) break;
+      P.fq_tail[q] = 0;
+      if (m.mode == KK_LEVEL_B) {
+        P.fq_kind[q] = 1;
+        P.fq_nst[q] = 1;
+        P.fq_off[q][0] = m.btab_off;
+        ok = mult(m.bmat, P.fq_k[q][0]);
+        if (m.btail) P.fq_tail[q] = 1;
+      } else {
+        P.fq_kind[q] = m.mode == KK_LEVEL_A ? 2 : 3;
+        P.fq_nst[q] = m.nstruct;
+        for (int s = 0; s < m.nstruct && ok; ++s) {
+          const KkComp& c = m.comp[s];
+          mult(c.mat, P.fq_k[q][s]);
+          P.fq_off[q][s] = c.tab_off;
+          if (P.fq_kind[q] == 2) ok = c.tab_off >= 0;
+          if (c.tail) P.fq_tail[q] |= 1 << s;
+        }
+      }
+    }
+    if (ok) {
+      P.fast_model = 3;
+      for (int k = 0; k < 9; ++k) P.fm[k] = c0.mat[k];
+      P.fm_ndim = mdl[0].ndim;
+    }
   }
 
   // ---- bucket by neighbour count

@@ -59,6 +59,12 @@ struct SolveParams {
   int fa_nst, fa_tailmask;   // Level A: structures, bit s = structure s has an analytic tail
   int fa_off[KK_FA_MAXS];    // their table offsets
   double fa_k[KK_FA_MAXS];   // and transform multiples
+  // fast_model 3 (2 variables, every structure's transform a multiple of fm):
+  // per pair i * 2 + j its kind (1 Level-B table, 2 Level-A tables, 3
+  // analytic), structures, table offsets, multiples and tail bits
+  int fq_kind[4], fq_nst[4], fq_tail[4];
+  int fq_off[4][KK_FA_MAXS];
+  double fq_k[4][KK_FA_MAXS];
 };
 
 enum {

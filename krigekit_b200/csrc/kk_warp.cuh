@@ -139,6 +139,35 @@ __device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs&
   return res;
 }
 
+// Two variables (P.fast_model == 3): COV(vgm(i, j), lag) at pair = 2 i + j from
+// that pair's Level-B table, its Level-A tables, or its analytic structures
+// (vgm(i, j), i > j, as the general model_cov evaluates it), every structure
+// at h_s = k_s * |fm lag|.
+__device__ __forceinline__ double fast_cov_pair(const SolveParams& P, const ZoneRegs& z, const double* lag,
+                                                int pair) {
+  const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
+  const int kind = P.fq_kind[pair];
+  if (kind == 1) {
+    const double hs = P.fq_k[pair][0] * h;
+    if (hs < z.zb3) return tab_fast(P.tables + P.fq_off[pair][0], z, hs);
+    return (P.fq_tail[pair] & 1) ? tail_cov(P.models + pair, hs) : 0.0;
+  }
+  double res = 0.0;
+  const int nst = P.fq_nst[pair];
+#pragma unroll
+  for (int s = 0; s < KK_FA_MAXS; ++s) {
+    if (s < nst) {
+      const double hs = P.fq_k[pair][s] * h;
+      double g;
+      if (kind == 3) g = comp_cov_h(P.models[pair].comp[s], hs);
+      else if (hs < z.zb3) g = tab_fast(P.tables + P.fq_off[pair][s], z, hs);
+      else g = ((P.fq_tail[pair] >> s) & 1) ? tail_comp(&P.models[pair].comp[s], hs) : 0.0;
+      res = dadd(res, g);
+    }
+  }
+  return res;
+}
+
 template <typename T, int N, bool REFINE>
 struct __align__(16) WarpSmem {
   double x[4][N];          // neighbour coordinates (nlag)
@@ -308,7 +337,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? fast_cov<FM>(P, zr, lag)
+        kv = fast ? (FM == 3 ? fast_cov_pair(P, zr, lag, vr * 2 + s.var[c]) : fast_cov<FM>(P, zr, lag))
                   : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
@@ -347,7 +376,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WS& s = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
   constexpr int NK = N * (N + 1) / 2;  // packed K64 of one target in Kg (from k_assemble)
-  const bool fast = P.fast_model != 0;
+  const bool fast = P.fast_model == 1 || P.fast_model == 2;  // right-hand side: one variable only
   const int lane = threadIdx.x & 31;
   const int pr = lane & 3, pc = lane >> 2;
   int n_items = nitems;
