@@ -605,6 +605,21 @@ void engine_solve(Engine& e) {
       for (int k = 0; k < 9; ++k) P.fm[k] = c0.mat[k];
       P.fm_ndim = m.ndim;
     }
+  } else if (e.st && nv == 1 && smdl[0].cs.mode == KK_LEVEL_B && smdl[0].ct.mode == KK_LEVEL_B &&
+             (smdl[0].model == 1 || !smdl[0].has_joint)) {
+    // space-time: spatial and temporal Level-B tables combined as product-sum
+    // (or sum-metric without joint sills), like the general st_cov
+    const KkSTModel& sm = smdl[0];
+    P.fast_model = 4;
+    for (int k = 0; k < 9; ++k) P.fm[k] = sm.cs.bmat[k];
+    P.fm_ndim = sm.cs.ndim;
+    P.fm_tail = sm.cs.btail;
+    P.fm_tab_off = sm.cs.btab_off;
+    P.ft_k = sm.ct.bmat[0];
+    P.ft_off = sm.ct.btab_off;
+    P.ft_tail = sm.ct.btail;
+    P.st_kind = sm.model;
+    P.st_kps = sm.k_ps;
   } else if (!e.st && nv == 2) {
     // two variables whose structures all have transforms k * B (structures
     // that differ only in range and sill, as in a linear model of

@@ -63,6 +63,11 @@ struct SolveParams {
   // per pair i * 2 + j its kind (1 Level-B table, 2 Level-A tables, 3
   // analytic), structures, table offsets, multiples and tail bits
   int fq_kind[4], fq_nst[4], fq_tail[4];
+  // fast_model 4 (space-time, one variable, Level-B spatial and temporal
+  // tables, product-sum or sum-metric without joint sills): the spatial
+  // table is fm / fm_tab_off / fm_tail, the temporal one ft_*
+  int ft_off, ft_tail, st_kind;
+  double ft_k, st_kps;
   int fq_off[4][KK_FA_MAXS];
   double fq_k[4][KK_FA_MAXS];
 };

@@ -1079,10 +1079,12 @@ void launch_assemble(const SolveParams& P, int N, const int* list, const int* cn
   if (N == 32) {
     if (P.fast_model == 2) k_assemble<32, 2><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else if (P.fast_model == 3) k_assemble<32, 3><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else if (P.fast_model == 4) k_assemble<32, 4><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else k_assemble<32, 1><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
   } else {
     if (P.fast_model == 2) k_assemble<64, 2><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else if (P.fast_model == 3) k_assemble<64, 3><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else if (P.fast_model == 4) k_assemble<64, 4><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else k_assemble<64, 1><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
   }
 }

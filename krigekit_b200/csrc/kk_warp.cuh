@@ -139,6 +139,22 @@ __device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs&
   return res;
 }
 
+// Space-time (P.fast_model == 4): st_cov of one variable from the spatial
+// table at |fm lag_s| and the temporal table at |ft_k dt| (dt = lag[P.ndim]),
+// combined in st_cov's order.
+__device__ __forceinline__ double fast_cov_st(const SolveParams& P, const ZoneRegs& z, const double* lag) {
+  const double hs = aniso_h_fast(P.fm, P.fm_ndim, lag);
+  const double dt = P.ndim == 1 ? lag[1] : (P.ndim == 2 ? lag[2] : lag[3]);
+  const double ht = fabs(P.ft_k * fabs(dt));
+  double cs, ct;
+  if (hs < z.zb3) cs = tab_fast(P.tables + P.fm_tab_off, z, hs);
+  else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
+  if (ht < z.zb3) ct = tab_fast(P.tables + P.ft_off, z, ht);
+  else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
+  if (P.st_kind == 1) return dadd(dadd(dmul(dmul(P.st_kps, cs), ct), cs), ct);
+  return dadd(cs, ct);
+}
+
 // Two variables (P.fast_model == 3): COV(vgm(i, j), lag) at pair = 2 i + j from
 // that pair's Level-B table, its Level-A tables, or its analytic structures
 // (vgm(i, j), i > j, as the general model_cov evaluates it), every structure
@@ -337,7 +353,9 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? (FM == 3 ? fast_cov_pair(P, zr, lag, vr * 2 + s.var[c]) : fast_cov<FM>(P, zr, lag))
+        kv = fast ? (FM == 3   ? fast_cov_pair(P, zr, lag, vr * 2 + s.var[c])
+                     : FM == 4 ? fast_cov_st(P, zr, lag)
+                               : fast_cov<FM>(P, zr, lag))
                   : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
