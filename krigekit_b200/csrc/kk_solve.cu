@@ -291,7 +291,16 @@ __device__ __noinline__ void finish_outputs(const SolveParams& P, int t, const d
 
 // Covariance of one neighbour row (coordinates xr, variable vr) with the
 // target for target variable iv, averaged over block nodes (assemble_rhs,
-// kriging.F90:889-910).
+// kriging.F90:889-910); defined after the fast covariance paths.
+__device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const double* xr, int vr, int iv, double rs);
+
+}  // namespace kk
+
+#include "kk_warp.cuh"
+
+namespace kk {
+
+// rhs_cov_row: the space-time fast path serves block nodes too
 __device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const double* xr, int vr, int iv, double rs) {
   double tmp = 0.0;
   if (P.gstart) {
@@ -300,20 +309,21 @@ __device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const do
       double node[4], lag[4];
       for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
       make_lag(P, xr, node, rs, lag);
-      tmp = dadd(tmp, dmul(cov_pair(P, vr, iv, lag), __ldg(&P.gw[k])));
+      const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+      tmp = dadd(tmp, dmul(cv, __ldg(&P.gw[k])));
     }
   } else {
     double node[4], lag[4];
     for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
     make_lag(P, xr, node, rs, lag);
-    tmp = dadd(tmp, dmul(cov_pair(P, vr, iv, lag), 1.0));
+    const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+    tmp = dadd(tmp, dmul(cv, 1.0));
   }
   return tmp;
 }
 
 }  // namespace kk
 
-#include "kk_warp.cuh"
 
 namespace kk {
 
