@@ -448,13 +448,18 @@ int krige_set_grid_drift(int64_t h, int ivar, int ndrift_c, int nblocks, const d
   if (e->ndrift == 0) throw std::string("grid/block drift is specified but ndrift==0");
   if (ndrift_c != e->ndrift) throw std::string("size(drift, 1) /= ndrift");
   if (nblocks != e->nblock) throw std::string("size(drift, 2) /= block%n; one drift value per block, not per grid node");
-  for (int ib = 0; ib < nblocks; ++ib)
-    for (int v = 0; v < e->nvar; ++v) {
-      if (ivar >= 1 && ivar != v + 1) continue;
-      if (ivar == 0 || ivar > e->nvar) throw std::string("ivar must be 1..nvar or < 0 (broadcast)");
-      for (int a = 0; a < ndrift_c; ++a)
-        e->bdrift[((size_t)ib * e->nvar + v) * e->ndrift + a] = drift[(size_t)ib * ndrift_c + a];
-    }
+  if (ivar == 0 || ivar > e->nvar) throw std::string("ivar must be 1..nvar or < 0 (broadcast)");
+  if (e->nvar == 1) {
+    // (ndrift, nblock) is already the (ndrift, nvar, nblock) layout
+    std::memcpy(e->bdrift.data(), drift, sizeof(double) * (size_t)nblocks * ndrift_c);
+  } else {
+    for (int ib = 0; ib < nblocks; ++ib)
+      for (int v = 0; v < e->nvar; ++v) {
+        if (ivar >= 1 && ivar != v + 1) continue;
+        for (int a = 0; a < ndrift_c; ++a)
+          e->bdrift[((size_t)ib * e->nvar + v) * e->ndrift + a] = drift[(size_t)ib * ndrift_c + a];
+      }
+  }
   KK_GUARD_END
 }
 
