@@ -1104,11 +1104,16 @@ void launch_factor(const SolveParams& P, int refine, int N, const int* list, con
   const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
   const bool narrow = C <= 3;
   if (refine) {
+    // the refinement's sweeps and residual cost in proportion to the columns
+    // carried: 3 (one variable, ordinary or simple), 5 (drift or two-variable
+    // cokriging), 6
     if (N == 32) {
       if (narrow) launch_warp<float, 32, true, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else if (C <= 5) launch_warp<float, 32, true, 5>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
       else launch_warp<float, 32, true, KK_REFINE_COLS>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
     } else {
       if (narrow) launch_warp<float, 64, true, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else if (C <= 5) launch_warp<float, 64, true, 5>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
       else launch_warp<float, 64, true, KK_REFINE_COLS>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
     }
   } else {
