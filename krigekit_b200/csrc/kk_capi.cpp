@@ -59,6 +59,31 @@ static void copy_d2h(void* dst, const void* src, size_t bytes) {
   if (err != cudaSuccess) throw std::string("CUDA error ") + cudaGetErrorString(err) + " reading results";
 }
 
+// Device results of a multi-variable solve into host memory for reordering:
+// the handle's pinned result buffer (kept across calls), or a caller-owned
+// vector when pinned memory cannot be had.
+static const double* results_to_host(Engine* e, const void* src, size_t n, std::vector<double>& fallback) {
+  const size_t bytes = sizeof(double) * n;
+  if (e->hres_bytes < bytes) {
+    if (e->hres) cudaFreeHost(e->hres);
+    e->hres = nullptr;
+    e->hres_bytes = 0;
+    if (cudaHostAlloc(&e->hres, bytes, cudaHostAllocPortable) == cudaSuccess) {
+      e->hres_bytes = bytes;
+    } else {
+      cudaGetLastError();
+      e->hres = nullptr;
+    }
+  }
+  if (e->hres) {
+    copy_d2h(e->hres, src, bytes);
+    return static_cast<const double*>(e->hres);
+  }
+  fallback.resize(n);
+  copy_d2h(fallback.data(), src, bytes);
+  return fallback.data();
+}
+
 static int vtype_id(const char* s) {
   // vtype_from_str, vgmfunc.f90:83-99 (case-insensitive 3-character prefix)
   static const char* names[] = {"nug", "sph", "exp", "gau", "hol", "pow", "bsq", "cir", "lin", "cyc", "dco"};
@@ -557,8 +582,8 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
     // est is (nblock) on the device: copy the first column straight into out
     copy_d2h(out, e->est.p, sizeof(double) * nblocks);
   } else {
-    std::vector<double> tmp((size_t)e->nblock * nv);
-    copy_d2h(tmp.data(), e->est.p, sizeof(double) * tmp.size());
+    std::vector<double> fb;
+    const double* tmp = results_to_host(e, e->est.p, (size_t)e->nblock * nv, fb);
     for (int iv = 0; iv < nvar_c; ++iv)
       for (int ib = 0; ib < nblocks; ++ib) out[ib + (size_t)nblocks * iv] = tmp[(size_t)ib * nv + iv];
   }
@@ -586,8 +611,8 @@ int krige_get_variance_all(int64_t h, int nblocks, int nvar_c, double* out) {
   if (nv == 1) {
     copy_d2h(out, e->var.p, sizeof(double) * nblocks);
   } else {
-    std::vector<double> tmp((size_t)e->nblock * nv * nv);
-    copy_d2h(tmp.data(), e->var.p, sizeof(double) * tmp.size());
+    std::vector<double> fb;
+    const double* tmp = results_to_host(e, e->var.p, (size_t)e->nblock * nv * nv, fb);
     for (int jv = 0; jv < nvar_c; ++jv)
       for (int iv = 0; iv < nvar_c; ++iv)
         for (int ib = 0; ib < nblocks; ++ib)

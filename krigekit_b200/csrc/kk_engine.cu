@@ -820,6 +820,9 @@ void engine_release(Engine& e) {
   if (e.hstage) cudaFreeHost(e.hstage);
   e.hstage = nullptr;
   e.hstage_bytes = 0;
+  if (e.hres) cudaFreeHost(e.hres);
+  e.hres = nullptr;
+  e.hres_bytes = 0;
 }
 
 }  // namespace kk

@@ -96,6 +96,8 @@ struct Engine {
   DBuf kbuf;  // packed K64 of one chunk of targets (assembly -> factorisation)
   DBuf til;  // point-target coordinates as given (nlag, nblock), before the per-axis split
   void* hstage = nullptr;  // pinned host staging for target uploads
+  void* hres = nullptr;    // pinned host staging for multi-variable results
+  size_t hres_bytes = 0;
   size_t hstage_bytes = 0;
   size_t scratch_bytes = 0;
   int mmax_total = 0;
