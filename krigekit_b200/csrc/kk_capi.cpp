@@ -556,7 +556,8 @@ int krige_get_block_coord(int64_t h, int ndim_c, int nblocks, double* out) {
   Engine* e = get(h);
   if (!e) return 1;
   const double* bc = e->bcoord_staged ? static_cast<const double*>(e->hstage) : e->bcoord.data();
-  if (!bc || (!e->bcoord_staged && e->bcoord.size() < (size_t)e->nblock * e->nlag))
+  if (nblocks > 0 && e->nblock > 0 &&
+      (!bc || (!e->bcoord_staged && e->bcoord.size() < (size_t)e->nblock * e->nlag)))
     throw std::string("no target coordinates are set");
   if (ndim_c > e->nlag) throw std::string("ndim exceeds the coordinate dimension of the targets");
   for (int ib = 0; ib < nblocks && ib < e->nblock; ++ib)

@@ -565,7 +565,9 @@ template <int CAP>
 __host__ __device__ inline SearchLayout search_layout(const KkSearch& S) {
   SearchLayout L;
   if (S.mode == 2) {
+    // at most KK_SEARCH_OCAP: a larger sector total takes the kd-tree path
     L.ocap = (((1 << S.ndim) * S.nmax + 1 + 31) / 32) * 32;
+    if (L.ocap > KK_SEARCH_OCAP) L.ocap = KK_SEARCH_OCAP;
     L.ocapd = 0;
   } else {
     L.ocap = (S.K + 1 + 31) / 32 * 32;
