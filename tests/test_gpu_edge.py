@@ -138,6 +138,25 @@ def test_sector_search_3d(precision):
     _check(g, o, float(np.std(z)), 1.02, TOL[precision])
 
 
+def test_sector_total_beyond_warp_buffers():
+    """3-D sector search with 8 x 48 neighbours: more than the warp search
+    keeps, so every target takes the exact kd-tree path (and the general
+    kernel, 384 > 64 rows)."""
+    x, z = _field(18, 5000, ndim=3)
+    grid = np.random.default_rng(10).uniform(0.2, 0.8, (40, 3))
+
+    def setup(k):
+        k.set_obs(1, x, z, nmax=48)
+        k.set_vgm(1, 1, "exp", nugget=0.05, sill=1.0, a_major=0.4)
+        k.set_grid(grid)
+        k.set_search(1, sector_search=True)
+        return k
+
+    g, o = _pair("fp64", setup, ndim=3, nvar=1)
+    _check(g, o, float(np.std(z)), 1.05, TOL["fp64"])
+    assert g.gpu_stats()["search_redo"] == len(grid)
+
+
 @pytest.mark.parametrize("precision", PRECISIONS)
 def test_rangescale_and_local_nugget(precision):
     x, z = _field(16, 2000)
