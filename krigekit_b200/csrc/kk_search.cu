@@ -428,7 +428,8 @@ __device__ void warp_sort_sec(double* key, int* idx, int n) {
 // falls between equal distances (the reference's heap order then decides:
 // the caller takes the exact kd-tree path); returns false when the boundary
 // buckets overflow bcap.
-__device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax, double dmax2, int bcap,
+template <class Pred>
+__device__ bool warp_select_sectors(const WarpBuf& b, int nk, Pred pred, int nsec, int nmax, double dmax2, int bcap,
                                     int* nout, bool* tie) {
   const int lane = threadIdx.x & 31;
   const int nbk = NBIN / nsec;                  // buckets per sector
@@ -437,6 +438,7 @@ __device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax
   __syncwarp();
   const double scale = dmax2 > 0.0 ? (double)nbk / dmax2 : 0.0;
   for (int j = lane; j < nk; j += 32) {
+    if (!pred(j)) continue;
     int q = (int)(b.d2[j] * scale);
     q = q < 0 ? 0 : (q >= nbk ? nbk - 1 : q);
     atomicAdd(&b.hist[b.sec[j] * nbk + q], 1);
@@ -493,14 +495,15 @@ __device__ bool warp_select_sectors(const WarpBuf& b, int nk, int nsec, int nmax
   for (int base = 0; base < nk; base += 32) {
     const int j = base + lane;
     int sj = 0, q = 0, bs = 0;
-    if (j < nk) {
+    const bool in = j < nk && pred(j);
+    if (in) {
       sj = b.sec[j];
       q = (int)(b.d2[j] * scale);
       q = q < 0 ? 0 : (q >= nbk ? nbk - 1 : q);
       bs = bsec[sj];
     }
-    const bool below = j < nk && q < bs;
-    const bool atb = j < nk && q == bs;
+    const bool below = in && q < bs;
+    const bool atb = in && q == bs;
     const unsigned lo = __ballot_sync(0xffffffffu, below);
     if (below) b.out[no + __popc(lo & lanemask_lt())] = b.idx[j];
     if (atb) {
@@ -852,26 +855,16 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
         } else {
           // sector filter (kriging.F90:1093-1154): within the K-set, the nmax
           // nearest of every sector among candidates within maxdist
-          // the K-set is every candidate with distance <= T (no tie at T);
-          // compact it, dropping the cross-validation target and points past maxdist
-          int nk = 0;
-          for (int base = 0; base < M; base += 32) {
-            int j = base + lane;
-            bool inset = j < M && B.d2[j] <= T && B.idx[j] != cvskip && B.d2[j] <= S.maxd2;
-            unsigned m = __ballot_sync(0xffffffffu, inset);
-            int p = nk + __popc(m & lanemask_lt());
-            double dv = inset ? B.d2[j] : 0.0;
-            int iv = inset ? B.idx[j] : 0;
-            signed char sv = inset ? B.sec[j] : 0;
-            __syncwarp();
-            if (inset) { B.d2[p] = dv; B.idx[p] = iv; B.sec[p] = sv; }
-            nk += __popc(m);
-            __syncwarp();
-          }
+          // the K-set is every candidate with distance <= T (no tie at T),
+          // without the cross-validation target and points past maxdist
+          const double* cd2 = B.d2;
+          const int* cidx = B.idx;
+          const double maxd2 = S.maxd2;
+          auto inset = [=](int j) { return cd2[j] <= T && cd2[j] <= maxd2 && cidx[j] != cvskip; };
           const int nsec = 1 << S.ndim;
           int nfin = 0;
           bool ties = false;
-          if (nsec * S.nmax >= OCAP || !warp_select_sectors(B, nk, nsec, S.nmax, T, BCAP, &nfin, &ties))
+          if (nsec * S.nmax >= OCAP || !warp_select_sectors(B, M, inset, nsec, S.nmax, T, BCAP, &nfin, &ties))
             st |= KK_ST_OVERFLOW;
           if (ties) st |= KK_ST_TIE;
           __syncwarp();
