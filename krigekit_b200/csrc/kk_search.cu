@@ -311,6 +311,33 @@ __device__ void warp_sort_ints(int* v, int n) {
   }
 }
 
+// Ascending bitonic sort of n2 = 32 or 64 ints held in registers, element i
+// in lane i % 32, register i / 32 (v0, v1): compare-exchange across lanes by
+// shuffle, across the two registers within a lane.
+__device__ __forceinline__ void warp_sort_reg64(int& v0, int& v1, int n2) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32) {  // partner is the other register of this lane
+        const bool up = ((lane & k) == 0);
+        const int lo = min(v0, v1), hi = max(v0, v1);
+        v0 = up ? lo : hi;
+        v1 = up ? hi : lo;
+        continue;
+      }
+      const bool lower = (lane & j) == 0;
+      const int o0 = __shfl_xor_sync(0xffffffffu, v0, j);
+      const bool up0 = ((lane & k) == 0);
+      v0 = (lower == up0) ? min(v0, o0) : max(v0, o0);
+      if (n2 == 64) {
+        const int o1 = __shfl_xor_sync(0xffffffffu, v1, j);
+        const bool up1 = (((32 + lane) & k) == 0);
+        v1 = (lower == up1) ? min(v1, o1) : max(v1, o1);
+      }
+    }
+  }
+}
+
 // Select the K smallest squared distances among candidates [0, M) for which
 // pred(j) holds; appends their (idx, d2) to out[*nout ...] when emit is set
 // (out and outd then hold at least *nout + K entries).  Returns the K-th
@@ -887,10 +914,19 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
     // isort: ascending observation index (kriging_base.F90:3209-3211)
     int np2 = 32;
     while (np2 < nsel) np2 <<= 1;
-    for (int i = nsel + lane; i < np2; i += 32) B.idx[i] = 0x7fffffff;
-    __syncwarp();
-    warp_sort_ints(B.idx, np2);
-    for (int i = lane; i < nsel; i += 32) nbr[(size_t)t * S.mmax + i] = B.idx[i];
+    if (np2 <= 64) {
+      // up to 64 indices: sorted in registers
+      int v0 = lane < nsel ? B.idx[lane] : 0x7fffffff;
+      int v1 = 32 + lane < nsel ? B.idx[32 + lane] : 0x7fffffff;
+      warp_sort_reg64(v0, v1, np2);
+      if (lane < nsel) nbr[(size_t)t * S.mmax + lane] = v0;
+      if (32 + lane < nsel) nbr[(size_t)t * S.mmax + 32 + lane] = v1;
+    } else {
+      for (int i = nsel + lane; i < np2; i += 32) B.idx[i] = 0x7fffffff;
+      __syncwarp();
+      warp_sort_ints(B.idx, np2);
+      for (int i = lane; i < nsel; i += 32) nbr[(size_t)t * S.mmax + i] = B.idx[i];
+    }
     if (lane == 0) { nnear[t] = nsel; status[t] = 0; }
     __syncwarp();
   }
