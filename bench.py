@@ -43,7 +43,7 @@ METRIC = "kriged targets/s on 1 B200: FP32+refine batched vs FP64 plain at <=1e-
 # search launch all 160 000 targets (coordinates and neighbour lists); both
 # grow in proportion to the targets.
 NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (1082.661e6 + 4.988e6) / 65536,
-                             "search": (8.640e6 + 1.391e6) / 160000}
+                             "search": (8.633e6 + 1.268e6) / 160000}
 
 
 def solve_flops(n, p=1, q=1):
