@@ -1056,7 +1056,7 @@ template <typename T, int N, bool REFINE, int CB>
 static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
                         const double* Kg, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
-  const size_t smem = sizeof(WarpSmem<T, N, REFINE>) * WPC;
+  const size_t smem = sizeof(WarpSmem<T, N, REFINE, CB>) * WPC;
   // per instantiation and device: function attributes belong to a context
   static bool attr_set[64] = {false};
   int dev = 0;

@@ -184,19 +184,19 @@ __device__ __forceinline__ double fast_cov_pair(const SolveParams& P, const Zone
   return res;
 }
 
-template <typename T, int N, bool REFINE>
+template <typename T, int N, bool REFINE, int CB>
 struct __align__(16) WarpSmem {
   double x[4][N];          // neighbour coordinates (nlag)
   double z[N];             // neighbour values
   int obs[N];
   int var[N];
   T col[2][4 * (N / 4 + (sizeof(T) == 8 ? 2 : 4))];  // column j of L, layout [pr][ri], padded rows
-  double ybc[2][MAXC];     // forward-substituted right-hand sides of row j
-  double G[MAXC * MAXC];
+  double ybc[2][CB];       // forward-substituted right-hand sides of row j
+  double G[CB * CB];
   double zmean[2 * KK_MAXVAR];
   float L[REFINE ? N * (N - 1) / 2 : 1];   // FP32 factor, strictly lower, packed by column
   float invd[REFINE ? N : 1];              // 1 / L[j][j]
-  double W[REFINE ? KK_REFINE_COLS * N : 1];         // current solution, broadcast for the residual
+  double W[REFINE ? CB * N : 1];           // current solution, broadcast for the residual
 };
 
 // start of column c of the strictly-lower packed factor
@@ -372,20 +372,22 @@ constexpr int warp_cta() { return 4; }
 
 // CTAs per SM the register budget is sized for (the launch bound caps the
 // registers at 64 K / (threads * this)): the FP64 N = 64 form needs the whole
-// register file of a lane for the matrix, the FP32 one fits in 168, the
-// N = 32 forms in 128
-template <typename T, int N, bool REFINE>
-constexpr int warp_min_ctas() { return N == 64 ? (REFINE ? 3 : 1) : 4; }
+// register file of a lane for the matrix; the FP32 one with three
+// right-hand-side columns fits in 128 registers and 55 KB of shared memory
+// per CTA (four CTAs per SM), the wider ones in 168 (three); the N = 32 forms
+// in 128
+template <typename T, int N, bool REFINE, int CB>
+constexpr int warp_min_ctas() { return N == 64 ? (REFINE ? (CB == 3 ? 4 : 3) : 1) : 4; }
 
 // CB: right-hand-side columns held per row at compile time (F | k | u);
 // 3 covers ordinary and simple kriging of one variable, the wider forms
 // cover drift and cokriging.
 template <typename T, int N, bool REFINE, int CB>
-__global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE>())
+__global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE, CB>())
     k_solve_warp(const __grid_constant__ SolveParams P, const int* __restrict__ list,
                  const int* __restrict__ list_count, int item0, int nitems, const double* __restrict__ Kg,
                  int work_slot) {
-  using WS = WarpSmem<T, N, REFINE>;
+  using WS = WarpSmem<T, N, REFINE, CB>;
   constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
   // column-buffer row stride: padded so the four row classes fall in
   // different banks and stay 16-byte aligned
