@@ -160,6 +160,12 @@ int krige_get_status(int64_t handle, int nblocks, int *status);
  * FP64 re-solves, refinement iterations; solve_ms = wall time of krige_solve. */
 int krige_gpu_stats(int64_t handle, int *out8, double *solve_ms);
 
+/* No counterpart in the reference.  Raw device counters of the last solve, out[0..n), n <= 32:
+ * [0..2] targets per size bucket (<= 32, 33..64, > 64 neighbours), [3] general-kernel
+ * list, [4] FP32 systems re-solved in FP64, [5] failures (NaN), [6] Cholesky solves,
+ * [7] LDL^T solves, [16..19] search fallbacks per variable, [20] refinement passes,
+ * [21] LDL^T solves that needed the 1e-6 mean-diagonal jitter. */
+int krige_gpu_counters(int64_t handle, int n, int *out);
 /* Enable per-phase CUDA-event timing of krige_solve (one event sync per phase). */
 int krige_gpu_profile(int64_t handle, int enable);
 /* Device ms per phase of the last solve: search, bucket, solve kernels, fallbacks;

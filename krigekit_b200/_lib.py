@@ -83,6 +83,7 @@ SIGNATURES = {
     "krige_get_mmax": ([_c_i64, _c_int, _p_int], _c_int),
     "krige_get_status": ([_c_i64, _c_int, _p_int], _c_int),
     "krige_gpu_stats": ([_c_i64, _p_int, _p_dbl], _c_int),
+    "krige_gpu_counters": ([_c_i64, _c_int, _p_int], _c_int),
     "krige_gpu_profile": ([_c_i64, _c_int], _c_int),
     "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),
     "krige_resolve_static": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),

@@ -6,6 +6,7 @@
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -33,7 +34,7 @@ def _run(cmd):
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS]
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
@@ -43,14 +44,18 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
                    "-Xcompiler", "-fPIC", "-rdc=false", "-c", s, "-o", o]
             if verbose_ptxas:
                 cmd.insert(1, "-Xptxas=-v")
-            _run(cmd)
+            cmds.append(cmd)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers + [__file__]):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
-                  "-I/usr/local/cuda/include", "-c", s, "-o", o])
+            cmds.append(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                         "-I/usr/local/cuda/include", "-c", s, "-o", o])
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, c) for c in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
     return LIB

@@ -710,6 +710,16 @@ int krige_gpu_stats(int64_t h, int* out8, double* solve_ms) {
   KK_GUARD_END
 }
 
+// Device counters of the last solve (KK_CNT_* of kk_kernels.h), n <= 32.
+int krige_gpu_counters(int64_t h, int n, int* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (n < 0 || n > KK_CNT_N_HOST) throw std::string("n must be 0..32");
+  for (int i = 0; i < n; ++i) out[i] = e->counters_last[i];
+  KK_GUARD_END
+}
+
 // Enable per-phase CUDA-event timing of solve() (adds one event sync per phase).
 int krige_gpu_profile(int64_t h, int enable) {
   KK_GUARD_BEGIN

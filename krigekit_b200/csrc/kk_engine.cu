@@ -23,6 +23,8 @@
 
 namespace kk {
 
+static_assert(KK_CNT_N_HOST == KK_CNT_N, "host copy of the device counters");
+
 static alloc_fn g_alloc = nullptr;
 static free_fn g_free = nullptr;
 static void* g_actx = nullptr;
@@ -747,6 +749,7 @@ void engine_solve(Engine& e) {
   e.stats[4] = 0;
   e.stats[6] = cnt[KK_CNT_FP64];
   e.stats[7] = cnt[KK_CNT_ITER];
+  std::memcpy(e.counters_last, cnt, sizeof cnt);
   if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");
   e.solved = true;
   e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -764,8 +767,9 @@ void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value) {
     if (ivar < 1 || ivar > e.nvar) throw std::string("ivar out of range");
     if (nobs != e.obs[ivar - 1].n) throw std::string("size(value) /= obs%n");
   }
-  KK_CUDA(cudaSetDevice(e.device));
-  cudaStream_t st = e.stream;
+  // Every check comes before the first change of state, so a rejected call
+  // leaves the handle's values and results as they were.
+  static_fit_check(e.mmax_total + e.pdrift(), e.nvar, e.pdrift());
   // the variogram may have been reset since the last solve: rebuild the
   // models on the host and copy them into the existing buffers when they fit
   std::vector<KkModel> mdl;
@@ -777,11 +781,19 @@ void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value) {
   const size_t mb = e.st ? sizeof(KkSTModel) * smdl.size() : sizeof(KkModel) * mdl.size();
   if (tb > e.tables.bytes || mb > e.models.bytes)
     throw std::string("the variogram tables outgrew the buffers of the last krige_solve; call krige_solve");
+  // the grid drift may have been replaced by krige_set_grid_drift since the
+  // last solve (same size: it is tied to the targets)
+  const size_t db = sizeof(double) * e.bdrift.size();
+  if (e.ndrift > 0 && db > e.tdrift.bytes)
+    throw std::string("the grid drift outgrew the buffer of the last krige_solve; call krige_solve");
+  KK_CUDA(cudaSetDevice(e.device));
+  cudaStream_t st = e.stream;
   e.solved = false;
   set_zones(st);
   KK_CUDA(cudaMemcpyAsync(e.tables.p, tabs.data(), tb, cudaMemcpyHostToDevice, st));
   KK_CUDA(cudaMemcpyAsync(e.models.p, e.st ? (const void*)smdl.data() : (const void*)mdl.data(), mb,
                           cudaMemcpyHostToDevice, st));
+  if (e.ndrift > 0 && db > 0) KK_CUDA(cudaMemcpyAsync(e.tdrift.p, e.bdrift.data(), db, cudaMemcpyHostToDevice, st));
   if (value) {
     ObsVar& o = e.obs[ivar - 1];
     std::copy(value, value + nobs, o.value.begin());
@@ -796,6 +808,7 @@ void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value) {
   e.stats[0] = cnt[KK_CNT_FAIL];
   e.stats[1] = cnt[KK_CNT_CHOL];
   e.stats[3] = cnt[KK_CNT_LDLT];
+  std::memcpy(e.counters_last, cnt, sizeof cnt);
   for (double& x : e.phase_ms) x = 0.0;
   e.launches = 2 * ((e.nblock + KK_STATIC_CHUNK - 1) / KK_STATIC_CHUNK);
   if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");

@@ -9,6 +9,8 @@
 
 #include "kk_common.h"
 
+#define KK_CNT_N_HOST 32  // = KK_CNT_N (kk_kernels.h)
+
 namespace kk {
 
 struct StructSpec {
@@ -103,6 +105,7 @@ struct Engine {
   int mmax_total = 0;
   bool solved = false;
   int stats[8] = {0};
+  int counters_last[KK_CNT_N_HOST] = {0};  // device counters of the last solve (KK_CNT_*)
   double last_solve_ms = 0.0;
   // per-phase device time of the last solve (CUDA events on the handle's
   // stream): search, bucket, solve kernels, fallbacks; and kernel launches

@@ -84,6 +84,7 @@ enum {
   KK_CNT_WORK0 = 8,  // persistent-kernel work counters (8..15)
   KK_CNT_REDO = 16,  // search tie/overflow count per variable (16..19)
   KK_CNT_ITER = 20,  // total refinement iterations
+  KK_CNT_JITTER = 21,  // LDL^T systems solved after the 1e-6 mean-diagonal jitter
   KK_CNT_N = 32
 };
 
@@ -129,5 +130,8 @@ constexpr int KK_STATIC_CHUNK = 1 << 16;  // targets per work-list chunk (two la
 // buffers; copies the counters of the run into cnt[KK_CNT_N] and
 // synchronises st.  The caller has made `device` current.
 void solve_generic_static(SolveParams P, int device, cudaStream_t st, int mtot, int* cnt);
+// Throws the same error as solve_generic_static when one system of mtot
+// equations does not fit in the static array (no device work).
+void static_fit_check(int mtot, int nv, int pa);
 
 }  // namespace kk

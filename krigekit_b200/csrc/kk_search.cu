@@ -933,7 +933,9 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
 }
 
 // ---------------------------------------------------------------------------
-// exact kd-tree replica for tie / overflow targets (one thread per target)
+// exact kd-tree replica for tie / overflow targets (one thread per target).
+// Its heap and visit order restate kdtree2 (M. Kennel 2004, Academic Free
+// License 1.1), which the reference bundles as kdtree2_maxidx.f90.
 // ---------------------------------------------------------------------------
 struct KdHeapEntry {
   double dis;

@@ -9,14 +9,13 @@
 //
 // Kernels here:
 //   k_bucket          npp per target -> size-bucket work lists
-//   k_solve_reg<..>   one CTA per target, thread i owns row i of K in
-//                     registers; right-looking Cholesky with one barrier per
-//                     column; right-hand sides forward-substituted in the
-//                     same sweep.  FP64: outputs from inner products of the
-//                     forward-substituted columns.  FP32: FP32 factor, FP64
-//                     refinement with K64 kept in shared memory.
-//   k_solve_generic   one thread per target in global workspace: n > 64,
-//                     Cholesky failures (Bunch-Kaufman LDL^T + jitter retry).
+//   k_assemble, k_solve_warp (kk_warp.cuh)
+//                     warp per target: covariance matrix, register Cholesky,
+//                     right-hand sides forward-substituted in the same sweep;
+//                     FP64, or FP32 factor with an FP64 residual correction
+//   k_solve_generic   one thread per target in global workspace: Cholesky
+//                     failures (Bunch-Kaufman LDL^T + jitter retry) and the
+//                     allocation-free re-solve
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -127,63 +126,11 @@ void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st) {
   k_bucket<<<(P.nblock + 255) / 256, 256, 0, st>>>(P, lists);
 }
 
-// ---------------------------------------------------------------------------
-// shared per-target preparation (gather + RHS) used by the register kernels
-// ---------------------------------------------------------------------------
-template <int NPAD>
-struct TargetSmem {
-  int obs[NPAD];
-  int var[NPAD];
-  double x[4][NPAD];
-  double z[NPAD];
-  int t, npp, nn[KK_MAXVAR], ist[KK_MAXVAR];
-  double rs, ln;
-};
-
 constexpr int MAXC = 8;  // forward-substituted columns: F + k + functionals (z, indicators)
 
 // number of functional columns carried for the estimate
 __device__ __forceinline__ int n_func(const SolveParams& P) {
   return 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
-}
-
-// value of functional column u at row r: z, then indicators of each variable
-template <int NPAD>
-__device__ __forceinline__ double u_entry(const TargetSmem<NPAD>& ts, int u, int r) {
-  if (u == 0) return ts.z[r];
-  return ts.var[r] == u - 1 ? 1.0 : 0.0;
-}
-
-// named barrier over the NT threads of this CTA
-template <int NT>
-__device__ __forceinline__ void group_sync() {
-  if (NT <= 32) __syncwarp();
-  else __syncthreads();
-}
-
-// Covariance of neighbour row r with the target (averaged over block nodes)
-// for target variable iv (assemble_rhs, kriging.F90:889-910).
-template <int NPAD>
-__device__ double rhs_cov(const SolveParams& P, const TargetSmem<NPAD>& ts, int r, int iv) {
-  double xr[4];
-  for (int d = 0; d < P.nlag; ++d) xr[d] = ts.x[d][r];
-  const int t = ts.t;
-  double tmp = 0.0;
-  if (P.gstart) {
-    const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
-    for (int k = k0; k < k1; ++k) {
-      double node[4], lag[4];
-      for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
-      make_lag(P, xr, node, ts.rs, lag);
-      tmp = dadd(tmp, dmul(cov_pair(P, ts.var[r], iv, lag), __ldg(&P.gw[k])));
-    }
-  } else {
-    double node[4], lag[4];
-    for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
-    make_lag(P, xr, node, ts.rs, lag);
-    tmp = dadd(tmp, dmul(cov_pair(P, ts.var[r], iv, lag), 1.0));
-  }
-  return tmp;
 }
 
 // prior covariance C_ij(x0, x0) for the variance (calc_variance,
@@ -326,361 +273,6 @@ __device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const do
 
 
 namespace kk {
-
-// ---------------------------------------------------------------------------
-// register kernel: one CTA of NPAD threads per target, thread i owns row i
-// ---------------------------------------------------------------------------
-template <typename T, int NPAD, bool REFINE>
-__global__ void __launch_bounds__(NPAD, 1) k_solve_reg(SolveParams P, const int* __restrict__ list,
-                                                     const int* __restrict__ list_count, int work_slot) {
-  constexpr int NT = NPAD;
-  constexpr int NK = NPAD * (NPAD + 1) / 2;
-  __shared__ TargetSmem<NPAD> ts;
-  __shared__ double Kp[NK];                 // K64 packed lower (row-major)
-  __shared__ __align__(16) T cb[2][NPAD + 16];  // column broadcast (double-buffered)
-  __shared__ double cols[MAXC][NPAD];       // forward-substituted columns / W
-  __shared__ double wvec[REFINE ? MAXC : 1][NPAD];  // raw F | k | u columns (refinement)
-  __shared__ double G[MAXC * MAXC];
-  __shared__ double zmean[2 * KK_MAXVAR];
-  __shared__ int s_item, s_flag;
-  __shared__ float Ls[REFINE ? NK : 1];     // FP32 factor (packed lower) for backward sweeps
-  __shared__ double red[2][NPAD / 32 + 1];
-
-  const int i = threadIdx.x;
-  const int n_items = *list_count;
-  const int nu = n_func(P);
-  const int C = P.pa + P.nvar + nu;
-
-  for (;;) {
-    if (i == 0) s_item = atomicAdd(&P.counters[work_slot], 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= n_items) break;
-    const int t = list[item];
-    // ---- gather neighbour rows (matrix order: variable blocks, ascending index)
-    if (i == 0) {
-      int acc = 0;
-      ts.t = t;
-      for (int v = 0; v < P.nvar; ++v) {
-        ts.nn[v] = P.nnear[v][t];
-        ts.ist[v] = acc;
-        acc += ts.nn[v];
-      }
-      ts.npp = acc;
-      ts.rs = P.rs ? P.rs[t] : 1.0;
-      ts.ln = P.ln ? P.ln[t] : 0.0;
-    }
-    __syncthreads();
-    const int npp = ts.npp;
-    if (i < npp) {
-      int v = 0;
-      while (v + 1 < P.nvar && i >= ts.ist[v + 1]) ++v;
-      int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (i - ts.ist[v])]);
-      ts.obs[i] = o;
-      ts.var[i] = v;
-      for (int d = 0; d < P.nlag; ++d) ts.x[d][i] = __ldg(&P.ox[v][d][o]);
-      ts.z[i] = __ldg(&P.oval[v][o]);
-    }
-    __syncthreads();
-    // ---- assemble K (assemble_lhs, kriging.F90:714-849): pairs balanced over threads
-    const int npairs = npp * (npp - 1) / 2;
-    for (int e = i; e < npairs; e += NT) {
-      int r = (int)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
-      while (r * (r - 1) / 2 > e) --r;
-      while ((r + 1) * r / 2 <= e) ++r;
-      int c = e - r * (r - 1) / 2;
-      double xc[4], xr[4], lag[4];
-      for (int d = 0; d < P.nlag; ++d) { xc[d] = ts.x[d][c]; xr[d] = ts.x[d][r]; }
-      make_lag(P, xc, xr, ts.rs, lag);
-      Kp[r * (r + 1) / 2 + c] = cov_pair(P, ts.var[r], ts.var[c], lag);
-    }
-    if (i < npp) {
-      const int v = ts.var[i];
-      double ov = __ldg(&P.ovar[v][ts.obs[i]]);
-      Kp[i * (i + 1) / 2 + i] = dadd(dadd(cov0_pair(P, v, v), ov), ts.ln);
-    }
-    // ---- right-hand-side columns for row i: F (pa), k (nvar), u (nu)
-    double b[MAXC];
-#pragma unroll
-    for (int c = 0; c < MAXC; ++c) b[c] = 0.0;
-    if (i < npp) {
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) {
-        if (c < P.pa) b[c] = f_entry(P, c, ts.var[i], ts.obs[i]);
-        else if (c < P.pa + P.nvar) b[c] = rhs_cov(P, ts, i, c - P.pa);
-        else if (!REFINE && c < C) b[c] = u_entry(ts, c - P.pa - P.nvar, i);
-      }
-    }
-    if (i == 0 && P.ck_isa) {
-      for (int v = 0; v < P.nvar; ++v) {
-        double s = 0.0;
-        for (int k = 0; k < ts.nn[v]; ++k) s = dadd(s, ts.z[ts.ist[v] + k]);
-        zmean[v] = ts.nn[v] > 0 ? s / ts.nn[v] : 0.0;
-        zmean[KK_MAXVAR + v] = (double)ts.nn[v];
-      }
-    }
-    __syncthreads();
-    // ---- load row i into registers (padding rows are identity)
-    T R[NPAD];
-#pragma unroll
-    for (int c = 0; c < NPAD; ++c) {
-      double v = 0.0;
-      if (i < npp) { if (c <= i) v = Kp[i * (i + 1) / 2 + c]; }
-      else if (c == i) v = 1.0;
-      R[c] = (T)v;
-    }
-    const int ncol = REFINE ? (P.pa + P.nvar) : C;
-    T y[MAXC];
-#pragma unroll
-    for (int c = 0; c < MAXC; ++c) y[c] = (T)b[c];
-    // warp-uniform bound on the row index of this warp
-    const int wmax = (i | 31) < npp - 1 ? (i | 31) : npp - 1;
-    if (i == 0) s_flag = 0;
-    // ---- right-looking Cholesky + forward substitution, one barrier per column
-#pragma unroll
-    for (int j = 0; j < NPAD; ++j) {
-      if (j >= npp) break;
-      T* cbj = cb[j & 1];
-      if (i >= j && i < npp) cbj[i] = R[j];
-      if (i == j) {
-        T d = R[j];
-        T inv;
-        if (!(d > (T)0)) { inv = (T)0; s_flag = 1; }
-        else inv = (T)1 / sqrt(d);
-        cbj[NPAD + MAXC] = inv;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < ncol) cbj[NPAD + c] = y[c];
-      }
-      __syncthreads();
-      if (s_flag) break;
-      const T inv = cbj[NPAD + MAXC];
-      if (i == j) {
-        R[j] = R[j] * inv;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < ncol) y[c] = y[c] * inv;
-      } else if (i > j && i < npp) {
-        const T li = R[j] * inv;
-        const T tt = li * inv;
-        R[j] = li;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < ncol) y[c] = y[c] - li * (cbj[NPAD + c] * inv);
-        if (j + 1 <= wmax) {
-#pragma unroll
-          for (int c = j + 1; c < NPAD; ++c) {
-            if (c > wmax) break;
-            if (c <= i) R[c] = R[c] - tt * cbj[c];
-          }
-        }
-      }
-    }
-    __syncthreads();
-    if (s_flag) {
-      // Cholesky failed: FP32 -> retry in FP64; FP64 -> generic LDL^T path
-      if (i == 0) {
-        if (REFINE) {
-          int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
-          P.fp64_list[p] = t;
-        } else {
-          int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
-          P.fb_list[p] = t;
-        }
-      }
-      __syncthreads();
-      continue;
-    }
-    if constexpr (!REFINE) {
-      // ---- FP64: inner products of the forward-substituted columns
-      if (i < npp) {
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < C) cols[c][i] = (double)y[c];
-      }
-      __syncthreads();
-      for (int pr = i; pr < C * C; pr += NT) {
-        int a = pr / C, bb = pr % C;
-        if (bb < a) continue;
-        double s = 0.0;
-        for (int r = 0; r < npp; ++r) s = fma(cols[a][r], cols[bb][r], s);
-        G[a * C + bb] = s;
-        G[bb * C + a] = s;
-      }
-      __syncthreads();
-      if (i == 0) {
-        int fail = 0;
-        finish_outputs(P, t, G, C, zmean, &fail);
-        if (fail) {
-          int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
-          P.fb_list[p] = t;
-        } else {
-          atomicAdd(&P.counters[KK_CNT_CHOL], 1);
-        }
-      }
-      __syncthreads();
-      continue;
-    } else {
-    // ---- FP32 + FP64 refinement (REFINE)
-    // keep L (FP32) in shared memory for backward sweeps
-    if (i < npp) {
-#pragma unroll
-      for (int c = 0; c < NPAD; ++c)
-        if (c <= i) Ls[i * (i + 1) / 2 + c] = (float)R[c];
-    }
-    const int nc = P.pa + P.nvar;
-    double W[MAXC];
-    // backward sweep: x = L^-T y (right-looking over columns of L^T)
-    {
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) W[c] = 0.0;
-      float yy[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) yy[c] = (float)y[c];
-      __syncthreads();
-      for (int j = npp - 1; j >= 0; --j) {
-        float* cbj = (float*)cb[j & 1];
-        if (i == j) {
-          const float ljj = Ls[j * (j + 1) / 2 + j];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) { yy[c] = yy[c] / ljj; cbj[c] = yy[c]; }
-        }
-        __syncthreads();
-        if (i < j) {
-          const float lji = Ls[j * (j + 1) / 2 + i];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) yy[c] = yy[c] - lji * cbj[c];
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) W[c] = c < nc ? (double)yy[c] : 0.0;
-    }
-    // refinement: r = b - K64 W (FP64), delta = K32^-1 r (FP32 sweeps)
-    int it = 0;
-    bool conv = false;
-    for (; it < 3; ++it) {
-      __syncthreads();
-      if (i < npp) {
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < nc) cols[c][i] = W[c];
-      }
-      __syncthreads();
-      double res[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) res[c] = (i < npp && c < nc) ? b[c] : 0.0;
-      if (i < npp) {
-        for (int m = 0; m < npp; ++m) {
-          const double kim = m <= i ? Kp[i * (i + 1) / 2 + m] : Kp[m * (m + 1) / 2 + i];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) res[c] = fma(-kim, cols[c][m], res[c]);
-        }
-      }
-      // forward sweep (L in shared memory), then backward sweep
-      float rr[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) rr[c] = (float)res[c];
-      for (int j = 0; j < npp; ++j) {
-        float* cbj = (float*)cb[j & 1];
-        if (i == j) {
-          const float ljj = Ls[j * (j + 1) / 2 + j];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) { rr[c] = rr[c] / ljj; cbj[c] = rr[c]; }
-        }
-        __syncthreads();
-        if (i > j && i < npp) {
-          const float lij = Ls[i * (i + 1) / 2 + j];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) rr[c] = rr[c] - lij * cbj[c];
-        }
-      }
-      for (int j = npp - 1; j >= 0; --j) {
-        float* cbj = (float*)cb[j & 1];
-        if (i == j) {
-          const float ljj = Ls[j * (j + 1) / 2 + j];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) { rr[c] = rr[c] / ljj; cbj[c] = rr[c]; }
-        }
-        __syncthreads();
-        if (i < j) {
-          const float lji = Ls[j * (j + 1) / 2 + i];
-#pragma unroll
-          for (int c = 0; c < MAXC; ++c)
-            if (c < nc) rr[c] = rr[c] - lji * cbj[c];
-        }
-      }
-      double dmax = 0.0, wmaxv = 0.0;
-      if (i < npp) {
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (c < nc) {
-            W[c] += (double)rr[c];
-            dmax = fmax(dmax, fabs((double)rr[c]));
-            wmaxv = fmax(wmaxv, fabs(W[c]));
-          }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-        wmaxv = fmax(wmaxv, __shfl_xor_sync(0xffffffffu, wmaxv, o));
-      }
-      __syncthreads();
-      if ((i & 31) == 0) { red[0][i >> 5] = dmax; red[1][i >> 5] = wmaxv; }
-      __syncthreads();
-      double dm = 0.0, wm = 0.0;
-      for (int q2 = 0; q2 < NT / 32 + (NT < 32 ? 1 : 0); ++q2) { dm = fmax(dm, red[0][q2]); wm = fmax(wm, red[1][q2]); }
-      if (dm <= P.refine_tol * wm) { conv = true; ++it; break; }
-    }
-    if (i == 0) atomicAdd(&P.counters[KK_CNT_ITER], it);
-    if (!conv) {
-      if (i == 0) {
-        int p = atomicAdd(&P.counters[KK_CNT_FP64], 1);
-        P.fp64_list[p] = t;
-      }
-      __syncthreads();
-      continue;
-    }
-    // ---- FP64 outputs from the refined W = K^-1 [F k]
-    __syncthreads();
-    if (i < npp) {
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c)
-        if (c < nc) { cols[c][i] = W[c]; wvec[c][i] = b[c]; }
-      for (int u = 0; u < nu; ++u) wvec[nc + u][i] = u_entry(ts, u, i);
-    }
-    __syncthreads();
-    // G in the FP64 layout: G[a][b] = col_a^T K^-1 col_b = col_a^T W_b for
-    // a in F|k|u, b in F|k
-    for (int pr = i; pr < C * C; pr += NT) {
-      int a = pr / C, bb = pr % C;
-      if (bb >= nc && a >= nc) { G[a * C + bb] = 0.0; continue; }
-      int wa = bb < nc ? bb : a;       // the W column index
-      int va = bb < nc ? a : bb;       // the raw vector index (0..C-1)
-      const double* vec = wvec[va];
-      double s = 0.0;
-      for (int r = 0; r < npp; ++r) s = fma(vec[r], cols[wa][r], s);
-      G[a * C + bb] = s;
-    }
-    __syncthreads();
-    if (i == 0) {
-      int fail = 0;
-      finish_outputs(P, t, G, C, zmean, &fail);
-      if (fail) {
-        int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
-        P.fb_list[p] = t;
-      } else {
-        atomicAdd(&P.counters[KK_CNT_CHOL], 1);
-      }
-    }
-    __syncthreads();
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // generic path: one thread per target, reference algorithm in global memory
@@ -977,6 +569,7 @@ __global__ void k_solve_generic(SolveParams P, const int* __restrict__ list, con
           for (int ii = 0; ii < npp; ++ii) A[ii + (size_t)ii * m] = A[ii + (size_t)ii * m] + dscale;
           for (size_t e = 0; e < (size_t)m * m; ++e) Af[e] = A[e];
           info = sytf2_u(m, Af, m, ipiv);
+          if (info == 0) atomicAdd(&P.counters[KK_CNT_JITTER], 1);
         }
       }
       if (info == 0) {
@@ -1044,14 +637,6 @@ __global__ void k_solve_generic(SolveParams P, const int* __restrict__ list, con
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <typename T, int NPAD, bool REFINE>
-static void launch_reg(const SolveParams& P, const int* list, const int* cnt, int slot, int nsm, cudaStream_t st) {
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_reg<T, NPAD, REFINE>, NPAD, 0);
-  if (occ < 1) occ = 1;
-  k_solve_reg<T, NPAD, REFINE><<<nsm * occ, NPAD, 0, st>>>(P, list, cnt, slot);
-}
-
 template <typename T, int N, bool REFINE, int CB>
 static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
                         const double* Kg, int slot, int nsm, cudaStream_t st) {
@@ -1174,7 +759,27 @@ static void static_check(cudaError_t err, const char* what) {
   if (err != cudaSuccess) throw std::string("CUDA error ") + cudaGetErrorString(err) + " at " + what;
 }
 
+// Workspace slots of the static array for systems of at most mtot equations;
+// throws when not even one target fits.
+static size_t static_slots(int mtot, int nv, int pa) {
+  const size_t ws_bytes = KK_STATIC_SCRATCH_BYTES - KK_STATIC_HEADER - KK_STATIC_LIST_BYTES;
+  const size_t stride = generic_stride(mtot, nv, pa);
+  const size_t slots = ws_bytes / (stride * sizeof(double));
+  if (slots < 1) {
+    char msg[256];
+    snprintf(msg, sizeof msg,
+             "krige_resolve_static: one target needs %zu bytes of workspace (%d equations), more than the %zu "
+             "bytes of static scratch; use krige_solve",
+             stride * sizeof(double), mtot, ws_bytes);
+    throw std::string(msg);
+  }
+  return slots;
+}
+
+void static_fit_check(int mtot, int nv, int pa) { static_slots(mtot, nv, pa); }
+
 void solve_generic_static(SolveParams P, int device, cudaStream_t st, int mtot, int* cnt) {
+  const size_t slots = static_slots(mtot, P.nvar, P.pa);
   std::lock_guard<std::mutex> lk(g_static_mu);
   if (device < 0 || device >= 64) throw std::string("device ordinal out of range for the static scratch");
   if (!g_static_addr[device]) {
@@ -1186,17 +791,7 @@ void solve_generic_static(SolveParams P, int device, cudaStream_t st, int mtot, 
     g_static_addr[device] = addr;
   }
   unsigned char* base = static_cast<unsigned char*>(g_static_addr[device]);
-  const size_t ws_bytes = KK_STATIC_SCRATCH_BYTES - KK_STATIC_HEADER - KK_STATIC_LIST_BYTES;
   const size_t stride = generic_stride(mtot, P.nvar, P.pa);
-  const size_t slots = ws_bytes / (stride * sizeof(double));
-  if (slots < 1) {
-    char msg[256];
-    snprintf(msg, sizeof msg,
-             "krige_resolve_static: one target needs %zu bytes of workspace (%d equations), more than the %zu "
-             "bytes of static scratch; use krige_solve",
-             stride * sizeof(double), mtot, ws_bytes);
-    throw std::string(msg);
-  }
   int* counters = reinterpret_cast<int*>(base);
   int* list_count = counters + KK_CNT_N;
   int* list = reinterpret_cast<int*>(base + KK_STATIC_HEADER);

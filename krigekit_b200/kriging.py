@@ -281,6 +281,14 @@ class Kriging:
         return {"fail": buf[0], "chol": buf[1], "ldlt": buf[3], "search_redo": buf[5],
                 "fp64_resolve": buf[6], "refine_iterations": buf[7], "solve_ms": ms.value}
 
+    def gpu_counters(self) -> dict:
+        """Raw device counters of the last solve (extension; krige_gpu_counters)."""
+        buf = (ctypes.c_int * 32)()
+        _lib.call("krige_gpu_counters", self._h(), 32, buf)
+        return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt64": buf[2], "general_list": buf[3],
+                "fp64_resolve": buf[4], "fail": buf[5], "chol": buf[6], "ldlt": buf[7],
+                "search_redo": [buf[16 + v] for v in range(4)], "refine_passes": buf[20], "jitter": buf[21]}
+
     def profile(self, enable: bool = True):
         """Record per-phase device time of each solve (extension)."""
         _lib.call("krige_gpu_profile", self._h(), int(bool(enable)))

@@ -21,11 +21,27 @@ TOL = 1e-9
 
 
 def _handle_pair(w):
+    if w.get("st"):
+        from krigekit_b200 import SpaceTimeKriging
+        a = bw.apply_st(SpaceTimeKriging(precision="fp64"), w)
+        b = bw.apply_st(SpaceTimeKriging(precision="fp64"), w)
+        return a, b
     from krigekit_b200 import Kriging
     kw = dict(ndim=w["ndim"], nvar=w["nvar"], **w["kw"])
     a = bw.apply(Kriging(precision="fp64", **kw), w)
     b = bw.apply(Kriging(precision="fp64", **kw), w)
     return a, b
+
+
+def _compare(a, b, zstd, sill, what):
+    e_s, v_s = _results(a)
+    e_r, v_r = _results(b)
+    assert np.array_equal(np.isnan(e_s), np.isnan(e_r))
+    ok = ~np.isnan(e_r)
+    ee = bw.rel_err(e_s[ok], e_r[ok], 1e-3 * zstd)
+    ve = bw.rel_err(v_s, v_r, 1e-3 * sill)
+    assert np.nanmax(ee) <= TOL, f"{what}: estimate rel err {np.nanmax(ee):.3e}"
+    assert np.nanmax(ve) <= TOL, f"{what}: variance rel err {np.nanmax(ve):.3e}"
 
 
 def _results(k):
@@ -67,15 +83,7 @@ def _check_two_calls(w, ivar):
         assert after == before, f"call {call}: {after - before} device allocations"
         b.update_obs_value(ivar, znew)
         b.solve()
-        e_s, v_s = _results(a)
-        e_r, v_r = _results(b)
-        assert np.array_equal(np.isnan(e_s), np.isnan(e_r))
-        ok = ~np.isnan(e_r)
-        zstd = float(np.std(znew))
-        ee = bw.rel_err(e_s[ok], e_r[ok], 1e-3 * zstd)
-        ve = bw.rel_err(v_s, v_r, 1e-3 * w["sill"])
-        assert np.nanmax(ee) <= TOL, f"call {call}: estimate rel err {np.nanmax(ee):.3e}"
-        assert np.nanmax(ve) <= TOL, f"call {call}: variance rel err {np.nanmax(ve):.3e}"
+        _compare(a, b, float(np.std(znew)), w["sill"], f"call {call}")
         assert a.solver_stats["fail"] == 0
     # null values: the same neighbour sets and values give the same results again
     e1, v1 = _results(a)
@@ -97,6 +105,50 @@ def test_resolve_static_cokriging():
     _check_two_calls(w, 2)
 
 
+def test_resolve_static_external_drift_changed_between_calls():
+    """KED (two external drifts): krige_set_grid_drift between the calls must
+    reach the re-solve, like it reaches the next krige_solve."""
+    from krigekit_b200 import _lib
+    w = bw.config3(grid_n=(12, 12, 4), nobs=3000)
+    a, b = _handle_pair(w)
+    a.solve()
+    b.solve()
+    gd0 = np.asarray(w["grid_drift"])
+    for call in range(2):
+        gd = gd0 * (1.0 + 0.3 * (call + 1)) + 0.05 * (call + 1)
+        a.set_grid_drift(gd)
+        b.set_grid_drift(gd)
+        assert _resolve_static(a, 0, None) == 0, _lib.last_error()
+        b.solve()
+        _compare(a, b, w["zstd"], w["sill"], f"drift call {call}")
+    a.close()
+    b.close()
+
+
+def test_resolve_static_space_time():
+    """Space-time product-sum model with block targets (krige_st_* handle)."""
+    w = bw.config5(grid_n=10, ntimes=3, nstations=120, ndays=40)
+    _check_two_calls(w, 1)
+
+
+def test_resolve_static_after_set_vgm():
+    """A variogram replaced between krige_solve and the re-solve (new sill and
+    range, same model shape): the re-solve rebuilds the tables in place."""
+    from krigekit_b200 import _lib
+    w = bw.config1(grid_n=20, nobs=600)
+    a, b = _handle_pair(w)
+    a.solve()
+    b.solve()
+    for call, (sill, rng_) in enumerate(((1.4, 0.18), (0.7, 0.33))):
+        for k in (a, b):
+            k.set_vgm(1, 1, "sph", nugget=0.05, sill=sill, a_major=rng_, append=False)
+        assert _resolve_static(a, 0, None) == 0, _lib.last_error()
+        b.solve()
+        _compare(a, b, w["zstd"], sill + 0.05, f"vgm call {call}")
+    a.close()
+    b.close()
+
+
 def test_resolve_static_rejects_oversized_systems():
     from krigekit_b200 import Kriging, _lib
     rng = np.random.default_rng(5)
@@ -108,8 +160,14 @@ def test_resolve_static_rejects_oversized_systems():
     k.set_grid(np.array([[0.5, 0.5]]))
     k.set_search(1)
     k.solve()
-    assert _resolve_static(k, 0, None) == 1
+    e0, v0 = _results(k)
+    z_new = np.cos(5 * obs[:, 1])
+    assert _resolve_static(k, 1, z_new) == 1
     assert "static scratch" in _lib.last_error()
+    # the rejected call changed nothing: the last solve's results stay readable
+    e1, v1 = _results(k)
+    np.testing.assert_array_equal(e0, e1)
+    np.testing.assert_array_equal(v0, v1)
     k.close()
 
 
