@@ -84,7 +84,7 @@ def _check_two_calls(w, ivar):
         b.update_obs_value(ivar, znew)
         b.solve()
         _compare(a, b, float(np.std(znew)), w["sill"], f"call {call}")
-        assert a.solver_stats["fail"] == 0
+        assert a.gpu_counters()["fail"] == 0
     # null values: the same neighbour sets and values give the same results again
     e1, v1 = _results(a)
     assert _resolve_static(a, 0, None) == 0, _lib.last_error()
