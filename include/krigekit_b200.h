@@ -28,8 +28,9 @@ int krige_create(int64_t *handle);
 int krige_destroy(int64_t *handle);
 
 /* kriging_capi.F90:143-192 krige_initialize -> initialize_base (kriging_base.F90:467-553).
- * nsim > 0, use_old_weight, store_weight, weight_correction and varying_vgm are
- * outside the GPU kriging path and return an error. */
+ * nsim > 0, weight_correction, varying_vgm and a non-empty weight_file are outside the
+ * GPU kriging path and return an error; store_weight / use_old_weight select the
+ * in-memory weight store (below). */
 int krige_initialize(int64_t handle, int ndim, int nvar, int ndrift, int unbias, int nsim,
                      int anisotropic_search, int weight_correction, int use_old_weight,
                      int store_weight, int cross_validation, int write_mat, int neglect_error,
@@ -78,6 +79,34 @@ int krige_solve(int64_t handle, int nthread, int ncache);
 void krige_solver_stats(int64_t handle, int *out);
 /* kriging_capi_common.F90:90-96 krige_get_last_error. */
 int krige_get_last_error(char *buffer, int nbuf);
+
+/* ---- weight store (in memory; kriging_base.F90:2703-2990, bound in the reference by
+ * src/krigekit/kriging.py:259-274).  krige_initialize with store_weight = 1 keeps the
+ * kriging weights and neighbour lists of the next krige_solve on the device (that solve
+ * runs the FP64 form); krige_update_obs_value then makes the next krige_solve a
+ * re-estimate from the stored weights (no search, no solve).  use_old_weight = 1 with
+ * krige_set_weights does the same with a caller's store.  Weight files are not written:
+ * weight_file must be empty.  Layouts are Fortran column-major; nm = the largest
+ * neighbour-list length (nmax, 2^ndim nmax with sectors, nobs when every observation
+ * is a neighbour), ng = nvar groups.  "Weight store not allocated" without a store. */
+/* krige_get_weight_dims: nm, ng = nvar, nb = nblocks. */
+int krige_get_weight_dims(int64_t handle, int *nm, int *ng, int *nb);
+/* nnear(ng, nb). */
+int krige_get_weight_nnear(int64_t handle, int ng, int nb, int *out);
+/* inear(nm, ng, nb), 1-based, zero past nnear. */
+int krige_get_weight_inear(int64_t handle, int nm, int ng, int nb, int *out);
+/* weight(nm, ng, nv, nb): weight of neighbour i of group g for target variable v. */
+int krige_get_weight_data(int64_t handle, int nm, int ng, int nv, int nb, double *out);
+/* var(nv, nv, nb): the conditional covariance stored with the weights. */
+int krige_get_weight_var(int64_t handle, int nv, int nb, double *out);
+/* Load a store (layouts as the getters; order(nb) is accepted and unused, var may be
+ * NULL for zero variances); the next krige_solve re-estimates from it. */
+int krige_set_weights(int64_t handle, int nm, int ng, int nv, int nb, const int *nnear, const int *inear,
+                      const double *weight, const int *order, const double *var);
+/* Release the store. */
+int krige_free_weight_store(int64_t handle);
+/* kriging_capi_common.F90 krige_to_str: configuration summary owned by the handle. */
+const char *krige_to_str(int64_t handle);
 
 /* kriging_capi_common.F90 krige_get_nblocks / krige_get_nsim. */
 int krige_get_nblocks(int64_t handle, int *nblocks);

@@ -87,6 +87,16 @@ SIGNATURES = {
     "krige_gpu_profile": ([_c_i64, _c_int], _c_int),
     "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),
     "krige_resolve_static": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
+    # in-memory weight store (reference layouts, kriging.py:259-274)
+    "krige_get_weight_dims": ([_c_i64, _p_int, _p_int, _p_int], _c_int),
+    "krige_get_weight_nnear": ([_c_i64, _c_int, _c_int, _p_int], _c_int),
+    "krige_get_weight_inear": ([_c_i64, _c_int, _c_int, _c_int, _p_int], _c_int),
+    "krige_get_weight_data": ([_c_i64, _c_int, _c_int, _c_int, _c_int, _p_dbl], _c_int),
+    "krige_get_weight_var": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
+    "krige_set_weights": ([_c_i64, _c_int, _c_int, _c_int, _c_int, _p_int, _p_int, _p_dbl, _p_int, _p_dbl],
+                          _c_int),
+    "krige_free_weight_store": ([_c_i64], _c_int),
+    "krige_to_str": ([_c_i64], ctypes.c_void_p),
 }
 
 _lib = None

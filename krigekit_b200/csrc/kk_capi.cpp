@@ -145,7 +145,10 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
   Engine* e = get(h);
   if (!e) return 1;
   if (nsim > 0) throw std::string("sequential simulation (nsim > 0) is not part of the GPU kriging path");
-  if (use_old_weight || store_weight) throw std::string("weight-file reuse is not part of the GPU kriging path");
+  if (store_weight && use_old_weight) throw std::string("store_weight and use_old_weight are mutually exclusive");
+  if ((store_weight || use_old_weight) && weight_file && weight_file[0])
+    throw std::string("weight files are not written by the GPU library: keep the weight store in memory "
+                      "(get_weights / set_weights)");
   if (weight_correction) throw std::string("weight_correction is not part of the GPU kriging path");
   if (varying_vgm) throw std::string("varying_vgm is not part of the GPU kriging path");
   if (ndim < 1 || ndim > 3) throw std::string("ndim must be 1, 2 or 3");
@@ -179,6 +182,9 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
   e->neglect_error = neglect_error;
   e->std_ck = std_ck;
   e->verbose = verbose;
+  engine_free_weight_store(*e);
+  e->store_weight = store_weight ? 1 : 0;
+  e->use_old_weight = use_old_weight ? 1 : 0;
   e->bounds[0] = bounds ? bounds[0] : -DBL_MAX;
   e->bounds[1] = bounds ? bounds[1] : DBL_MAX;
   e->obs.assign(nvar, ObsVar());
@@ -255,6 +261,12 @@ int krige_update_obs_value(int64_t h, int ivar, int nobs, const double* value) {
   bool keep_search = o.search_set;
   o.dirty = true;
   o.search_set = keep_search;
+  // with a complete weight store the next solve reuses the weights
+  // (update_obs_value_base, kriging_base.F90:669-677)
+  if (e->wstore_dev && e->solved) {
+    e->use_old_weight = 1;
+    e->store_weight = 0;
+  }
   KK_GUARD_END
 }
 
@@ -708,6 +720,111 @@ int krige_gpu_stats(int64_t h, int* out8, double* solve_ms) {
   for (int i = 0; i < 8; ++i) out8[i] = e->stats[i];
   if (solve_ms) *solve_ms = e->last_solve_ms;
   KK_GUARD_END
+}
+
+// ---- weight store (kriging_capi_common.F90 weight-store entry points,
+// kriging_base.F90:2703-2990); layouts as the reference's ctypes binding
+// (kriging.py:259-274)
+int krige_get_weight_dims(int64_t h, int* nm, int* ng, int* nb) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (!e->wstore_dev && !e->wstore_host) throw std::string("Weight store not allocated. Set store_weight=True.");
+  *nm = engine_weight_nm(*e);
+  *ng = e->nvar;
+  *nb = e->nblock;
+  KK_GUARD_END
+}
+
+int krige_get_weight_nnear(int64_t h, int ng, int nb, int* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_get_weights(*e, engine_weight_nm(*e), ng, e->nvar, nb, out, nullptr, nullptr, nullptr);
+  KK_GUARD_END
+}
+
+int krige_get_weight_inear(int64_t h, int nm, int ng, int nb, int* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_get_weights(*e, nm, ng, e->nvar, nb, nullptr, out, nullptr, nullptr);
+  KK_GUARD_END
+}
+
+int krige_get_weight_data(int64_t h, int nm, int ng, int nv, int nb, double* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_get_weights(*e, nm, ng, nv, nb, nullptr, nullptr, out, nullptr);
+  KK_GUARD_END
+}
+
+int krige_get_weight_var(int64_t h, int nv, int nb, double* out) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_get_weights(*e, engine_weight_nm(*e), e->nvar, nv, nb, nullptr, nullptr, nullptr, out);
+  KK_GUARD_END
+}
+
+int krige_set_weights(int64_t h, int nm, int ng, int nv, int nb, const int* nnear, const int* inear,
+                      const double* weight, const int* order, const double* var) {
+  (void)order;  // the visiting order only matters for sequential simulation
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_set_weights(*e, nm, ng, nv, nb, nnear, inear, weight, var);
+  KK_GUARD_END
+}
+
+int krige_free_weight_store(int64_t h) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  engine_free_weight_store(*e);
+  KK_GUARD_END
+}
+
+// Configuration summary (to_str_base, kriging_base.F90:3601-3646); the text
+// belongs to the handle and stays valid until the next call on it.
+const char* krige_to_str(int64_t h) {
+  Engine* e = get(h);
+  if (!e) return nullptr;
+  auto yn = [](int b) { return b ? "yes" : "no"; };
+  char buf[256];
+  std::string r = "\n==================== Configuration ====================\n";
+  auto line = [&](const char* k, const std::string& v) { r += " "; r += k; r += " : " + v + "\n"; };
+  line("Engine                ", "B200 (sm_100a) kriging solve path");
+  line("Dimension             ", std::to_string(e->ndim));
+  line("Number of Variables   ", std::to_string(e->nvar));
+  line("Number of Simulations ", std::to_string(e->nsim));
+  line("Number of Drifts      ", std::to_string(e->ndrift));
+  line("Number of Blocks      ", std::to_string(e->nblock));
+  line("Ordinary Kriging      ", yn(e->unbias == 1));
+  line("Standard CoKriging    ", yn(e->std_ck));
+  line("LOO-Cross Validation  ", yn(e->cross_validation));
+  line("Use Old Weights       ", yn(e->use_old_weight));
+  line("Store Weights         ", yn(e->store_weight));
+  line("Precision             ", e->precision ? "FP32 factor + FP64 correction" : "FP64");
+  snprintf(buf, sizeof buf, "%.17g", e->bounds[0]);
+  line("Lower Bound           ", buf);
+  snprintf(buf, sizeof buf, "%.17g", e->bounds[1]);
+  line("Upper Bound           ", buf);
+  for (int v = 0; v < (int)e->obs.size(); ++v) {
+    const ObsVar& o = e->obs[v];
+    r += "Variable " + std::to_string(v + 1) + ":\n";
+    line("Number of data        ", std::to_string(o.n));
+    line("Maximum neighbors     ", std::to_string(o.nmax));
+    snprintf(buf, sizeof buf, "%.17g", o.maxdist);
+    line("Maxdist               ", buf);
+    snprintf(buf, sizeof buf, "%.17g", o.sk_mean);
+    line("Simple Kriging Mean   ", buf);
+    line("Sector Search         ", yn(o.sector));
+  }
+  r += "================== End Configuration ==================\n";
+  e->info = r;
+  return e->info.c_str();
 }
 
 // Device counters of the last solve (KK_CNT_* of kk_kernels.h), n <= 32.

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -392,13 +393,22 @@ static void fill_params(Engine& e, SolveParams& P) {
     throw std::string("too many drift/variable columns for the register kernels (max 8)");
 }
 
+static void engine_replay(Engine& e);
+
 void engine_solve(Engine& e) {
   auto t0 = std::chrono::steady_clock::now();
   for (double& x : e.phase_ms) x = 0.0;
   e.launches = 0;
   e.solved = false;
   std::memset(e.stats, 0, sizeof e.stats);
+  if (e.use_old_weight) {
+    // weight-store reuse: no search and no solve (load_block_weights)
+    engine_replay(e);
+    e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return;
+  }
   validate(e);
+  e.wstore_dev = false;  // this solve's neighbour lists replace the store's
   KK_CUDA(cudaSetDevice(e.device));
   PhaseTimer timer(e);
   cudaStream_t st = e.stream;
@@ -682,7 +692,15 @@ void engine_solve(Engine& e) {
   KK_CUDA(cudaStreamSynchronize(st));
   // ---- solve: per chunk of a bucket list, the assembly kernel writes packed
   // K64 to kbuf, then the factorisation kernel reads it
-  const int refine = solve_refine_form(P, e.precision);
+  if (e.store_weight) {
+    // the weight store is filled by the FP64 form and the general kernel
+    e.wstride = mm_total;
+    for (int v = 0; v < nv; ++v) e.wmmax[v] = P.mmax[v];
+    e.wbuf.reserve(sizeof(double) * (size_t)nb * nv * std::max(mm_total, 1));
+    P.wout = e.wbuf.as<double>();
+    P.wstride = mm_total;
+  }
+  const int refine = e.store_weight ? 0 : solve_refine_form(P, e.precision);
   constexpr int CH = 1 << 16;
   const int nk64 = 64 * 65 / 2;
   const int most = std::max(cb[KK_CNT_B16], cb[KK_CNT_B64]);
@@ -708,7 +726,7 @@ void engine_solve(Engine& e) {
     KK_CUDA(cudaMemcpyAsync(&nf, e.counters.as<int>() + KK_CNT_FP64, sizeof(int), cudaMemcpyDeviceToHost, st));
     KK_CUDA(cudaStreamSynchronize(st));
     if (nf > 0) {
-      e.kbuf.reserve(sizeof(double) * (size_t)std::min(CH, nf) * nk64);
+      e.kbuf.reserve(std::max(e.kbuf.bytes, sizeof(double) * (size_t)std::min(CH, nf) * nk64));
       timer.start();
       run_list(P.fp64_list, nf, 64, 0, KK_CNT_WORK0 + 2);
       timer.stop(3);
@@ -751,6 +769,10 @@ void engine_solve(Engine& e) {
   e.stats[7] = cnt[KK_CNT_ITER];
   std::memcpy(e.counters_last, cnt, sizeof cnt);
   if (!e.neglect_error && cnt[KK_CNT_FAIL] > 0) throw std::string("Singular matrix or no neighbours at a block");
+  if (e.store_weight) {
+    e.wstore_dev = true;
+    e.wstore_host = false;
+  }
   e.solved = true;
   e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -815,6 +837,212 @@ void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value) {
   e.solved = true;
 }
 
+// Neighbour-list length of every variable as the next solve would set it
+// (set_search must have been called for the search mode; the default is the
+// plain k-nearest search).
+static void list_lengths(Engine& e, int* mm) {
+  for (int v = 0; v < e.nvar; ++v) {
+    KkSearch S;
+    setup_search(e, v, S);
+    mm[v] = std::max(S.mmax, 1);
+  }
+}
+
+int engine_weight_nm(Engine& e) {
+  int mm[KK_MAXVAR] = {0, 0, 0, 0};
+  if (e.wstore_dev || e.wstore_host) std::memcpy(mm, e.wmmax, sizeof mm);
+  else list_lengths(e, mm);
+  int nm = 0;
+  for (int v = 0; v < e.nvar; ++v) nm = std::max(nm, mm[v]);
+  return nm;
+}
+
+// Estimates from the weight store (use_old_weight): the observation values
+// of every variable are uploaded (update_obs_value may have replaced them),
+// a store staged by set_weights is uploaded once, then one gather-dot kernel
+// writes the estimates; the variances are the store's.
+static void engine_replay(Engine& e) {
+  if (!e.wstore_dev && !e.wstore_host)
+    throw std::string("use_old_weight with no weight_file requires set_weights() to be called first.");
+  if (e.nblock <= 0) throw std::string("Call set_grid() before solve().");
+  for (int v = 0; v < e.nvar; ++v)
+    if (e.obs[v].n == 0) throw std::string("Call set_obs() for every variable before solve().");
+  KK_CUDA(cudaSetDevice(e.device));
+  cudaStream_t st = e.stream;
+  const int nb = e.nblock, nv = e.nvar;
+  for (int v = 0; v < nv; ++v)
+    upload(e.vd[v].value, e.obs[v].value.data(), sizeof(double) * e.obs[v].n, st);
+  e.est.reserve(sizeof(double) * (size_t)nb * nv);
+  e.var.reserve(sizeof(double) * (size_t)nb * nv * nv);
+  e.status.reserve(sizeof(int) * nb);
+  if (e.wstore_host) {
+    const int ng = nv, nm = e.wh_nm;
+    std::vector<int> nn((size_t)nb), nbr;
+    std::vector<double> w((size_t)nb * nv * e.wstride, 0.0);
+    std::vector<int> ist((size_t)nb * nv, 0);
+    for (int ib = 0; ib < nb; ++ib)
+      for (int v = 1; v < nv; ++v)
+        ist[(size_t)ib * nv + v] = ist[(size_t)ib * nv + v - 1] + e.wh_nnear[(size_t)(v - 1) + (size_t)ng * ib];
+    for (int v = 0; v < nv; ++v) {
+      const int mm = e.wmmax[v];
+      nbr.assign((size_t)nb * mm, 0);
+      for (int ib = 0; ib < nb; ++ib) {
+        const int k = e.wh_nnear[(size_t)v + (size_t)ng * ib];
+        nn[ib] = k;
+        for (int i = 0; i < k; ++i) {
+          nbr[(size_t)ib * mm + i] = e.wh_inear[(size_t)i + (size_t)nm * (v + (size_t)ng * ib)] - 1;
+          for (int jv = 0; jv < nv; ++jv)
+            w[((size_t)ib * nv + jv) * e.wstride + ist[(size_t)ib * nv + v] + i] =
+                e.wh_weight[(size_t)i + (size_t)nm * (v + (size_t)ng * (jv + (size_t)nv * ib))];
+        }
+      }
+      upload(e.vd[v].nnear, nn.data(), sizeof(int) * nb, st);
+      upload(e.vd[v].nbr, nbr.data(), sizeof(int) * nbr.size(), st);
+      KK_CUDA(cudaStreamSynchronize(st));
+    }
+    upload(e.wbuf, w.data(), sizeof(double) * w.size(), st);
+    // variance(nvar, nvar, nblock) -> per target [iv + jv nvar]
+    std::vector<double> vv((size_t)nb * nv * nv);
+    for (int ib = 0; ib < nb; ++ib)
+      for (int jv = 0; jv < nv; ++jv)
+        for (int iv = 0; iv < nv; ++iv)
+          vv[((size_t)ib * nv + jv) * nv + iv] = e.wh_var[(size_t)iv + (size_t)nv * (jv + (size_t)nv * ib)];
+    KK_CUDA(cudaMemcpyAsync(e.var.p, vv.data(), sizeof(double) * vv.size(), cudaMemcpyHostToDevice, st));
+    KK_CUDA(cudaMemsetAsync(e.status.p, 0, sizeof(int) * nb, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    e.wstore_host = false;
+    e.wstore_dev = true;
+    e.wh_nnear.clear(); e.wh_inear.clear(); e.wh_weight.clear(); e.wh_var.clear();
+  }
+  SolveParams P;
+  std::memset(&P, 0, sizeof P);
+  P.nvar = nv;
+  P.nblock = nb;
+  P.unbias = e.unbias;
+  P.ck_isa = (!e.std_ck && e.unbias != 0 && nv > 1) ? 1 : 0;
+  P.bounds[0] = e.bounds[0];
+  P.bounds[1] = e.bounds[1];
+  for (int v = 0; v < nv; ++v) {
+    P.sk_mean[v] = e.obs[v].sk_mean;
+    P.oval[v] = e.vd[v].value.as<double>();
+    P.nbr[v] = e.vd[v].nbr.as<int>();
+    P.nnear[v] = e.vd[v].nnear.as<int>();
+    P.mmax[v] = e.wmmax[v];
+    P.nobs[v] = e.obs[v].n;
+  }
+  P.est = e.est.as<double>();
+  P.var = e.var.as<double>();
+  P.status = e.status.as<int>();
+  P.wout = e.wbuf.as<double>();
+  P.wstride = e.wstride;
+  launch_replay(P, sm_count(e.device), st);
+  KK_CUDA(cudaGetLastError());
+  KK_CUDA(cudaStreamSynchronize(st));
+  e.launches = 1;
+  std::memset(e.counters_last, 0, sizeof e.counters_last);
+  e.solved = true;
+}
+
+void engine_set_weights(Engine& e, int nm, int ng, int nv, int nb, const int* nnear, const int* inear,
+                        const double* weight, const double* var) {
+  if (e.obs.empty() || e.obs[0].n == 0) throw std::string("call set_obs() before set_weights() so nmax is set");
+  if (nb != e.nblock || ng != e.nvar) throw std::string("nnear shape mismatch");
+  int mm[KK_MAXVAR] = {0, 0, 0, 0};
+  list_lengths(e, mm);
+  int nmx = 0;
+  for (int v = 0; v < e.nvar; ++v) nmx = std::max(nmx, mm[v]);
+  if (nm != nmx) throw std::string("inear shape mismatch");
+  if (nv != e.nvar) throw std::string("weight shape mismatch");
+  for (int ib = 0; ib < nb; ++ib)
+    for (int v = 0; v < ng; ++v) {
+      const int k = nnear[(size_t)v + (size_t)ng * ib];
+      if (k < 0 || k > mm[v]) throw std::string("nnear exceeds the neighbour-list length of its variable");
+      for (int i = 0; i < k; ++i) {
+        const int o = inear[(size_t)i + (size_t)nm * (v + (size_t)ng * ib)];
+        if (o < 1 || o > e.obs[v].n) throw std::string("inear holds an index outside 1..nobs");
+      }
+    }
+  e.wh_nm = nm;
+  e.wh_nnear.assign(nnear, nnear + (size_t)ng * nb);
+  e.wh_inear.assign(inear, inear + (size_t)nm * ng * nb);
+  e.wh_weight.assign(weight, weight + (size_t)nm * ng * nv * nb);
+  if (var) e.wh_var.assign(var, var + (size_t)nv * nv * nb);
+  else e.wh_var.assign((size_t)nv * nv * nb, 0.0);
+  std::memcpy(e.wmmax, mm, sizeof mm);
+  e.wstride = 0;
+  for (int v = 0; v < e.nvar; ++v) e.wstride += mm[v];
+  e.wstore_host = true;
+  e.wstore_dev = false;
+  e.use_old_weight = 1;
+  e.solved = false;
+}
+
+void engine_get_weights(Engine& e, int nm, int ng, int nv, int nb, int* nnear, int* inear, double* weight,
+                        double* var) {
+  if (!e.wstore_dev && !e.wstore_host) throw std::string("Weight store not allocated. Set store_weight=True.");
+  if (nb != e.nblock || ng != e.nvar || nv != e.nvar || nm != engine_weight_nm(e))
+    throw std::string("weight store dimensions do not match the buffers");
+  if (e.wstore_host) {
+    if (nnear) std::copy(e.wh_nnear.begin(), e.wh_nnear.end(), nnear);
+    if (inear) std::copy(e.wh_inear.begin(), e.wh_inear.end(), inear);
+    if (weight) std::copy(e.wh_weight.begin(), e.wh_weight.end(), weight);
+    if (var) std::copy(e.wh_var.begin(), e.wh_var.end(), var);
+    return;
+  }
+  KK_CUDA(cudaSetDevice(e.device));
+  cudaStream_t st = e.stream;
+  std::vector<std::vector<int>> nn(nv), nbr(nv);
+  for (int v = 0; v < nv; ++v) {
+    nn[v].resize(nb);
+    KK_CUDA(cudaMemcpyAsync(nn[v].data(), e.vd[v].nnear.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    if (inear || weight) {
+      nbr[v].resize((size_t)nb * e.wmmax[v]);
+      KK_CUDA(cudaMemcpyAsync(nbr[v].data(), e.vd[v].nbr.p, sizeof(int) * nbr[v].size(), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  std::vector<double> w;
+  if (weight) {
+    w.resize((size_t)nb * nv * e.wstride);
+    KK_CUDA(cudaMemcpyAsync(w.data(), e.wbuf.p, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, st));
+  }
+  std::vector<double> vv;
+  if (var) {
+    vv.resize((size_t)nb * nv * nv);
+    KK_CUDA(cudaMemcpyAsync(vv.data(), e.var.p, sizeof(double) * vv.size(), cudaMemcpyDeviceToHost, st));
+  }
+  KK_CUDA(cudaStreamSynchronize(st));
+  // unused slots are zero (test_weight_store.py: padding checks)
+  if (inear) std::fill(inear, inear + (size_t)nm * ng * nb, 0);
+  if (weight) std::fill(weight, weight + (size_t)nm * ng * nv * nb, 0.0);
+  for (int ib = 0; ib < nb; ++ib) {
+    int ist = 0;
+    for (int v = 0; v < ng; ++v) {
+      const int k = nn[v][ib];
+      if (nnear) nnear[(size_t)v + (size_t)ng * ib] = k;
+      for (int i = 0; i < k; ++i) {
+        if (inear) inear[(size_t)i + (size_t)nm * (v + (size_t)ng * ib)] = nbr[v][(size_t)ib * e.wmmax[v] + i] + 1;
+        if (weight)
+          for (int jv = 0; jv < nv; ++jv)
+            weight[(size_t)i + (size_t)nm * (v + (size_t)ng * (jv + (size_t)nv * ib))] =
+                w[((size_t)ib * nv + jv) * e.wstride + ist + i];
+      }
+      ist += k;
+    }
+    if (var)
+      for (int jv = 0; jv < nv; ++jv)
+        for (int iv = 0; iv < nv; ++iv)
+          var[(size_t)iv + (size_t)nv * (jv + (size_t)nv * ib)] = vv[((size_t)ib * nv + jv) * nv + iv];
+  }
+}
+
+void engine_free_weight_store(Engine& e) {
+  e.wbuf.release();
+  e.wh_nnear.clear(); e.wh_inear.clear(); e.wh_weight.clear(); e.wh_var.clear();
+  e.wstore_dev = false;
+  e.wstore_host = false;
+  e.use_old_weight = 0;
+}
+
 void engine_release(Engine& e) {
   for (int v = 0; v < KK_MAXVAR; ++v) {
     VarDevice& d = e.vd[v];
@@ -829,7 +1057,7 @@ void engine_release(Engine& e) {
   for (auto& b : e.gx) b.release();
   e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
   e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
-  e.counters.release(); e.scratch.release(); e.kbuf.release(); e.til.release();
+  e.counters.release(); e.scratch.release(); e.kbuf.release(); e.til.release(); e.wbuf.release();
   if (e.hstage) cudaFreeHost(e.hstage);
   e.hstage = nullptr;
   e.hstage_bytes = 0;

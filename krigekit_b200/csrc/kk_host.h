@@ -113,6 +113,24 @@ struct Engine {
   double phase_ms[4] = {0, 0, 0, 0};
   int launches = 0;
 
+  // weight store (store_weight / use_old_weight, kriging_base.F90:2703-2990):
+  // the weights of every target stay on the device after a store_weight
+  // solve, wbuf[(t * nvar + jv) * wstride + row] with rows in matrix order,
+  // together with the neighbour lists of that solve; set_weights stages a
+  // caller's store on the host until the next solve uploads it
+  int store_weight = 0, use_old_weight = 0;
+  bool wstore_dev = false;   // the device holds a complete store
+  bool wstore_host = false;  // set_weights data waiting for upload
+  int wstride = 0;           // weight rows per target variable (sum of mmax)
+  int wmmax[KK_MAXVAR] = {0, 0, 0, 0};  // neighbour-list stride per variable of the store
+  DBuf wbuf;
+  std::vector<int> wh_nnear;      // (ngroups, nblock)
+  std::vector<int> wh_inear;      // (nm, ngroups, nblock), 1-based
+  std::vector<double> wh_weight;  // (nm, ngroups, nvar, nblock)
+  std::vector<double> wh_var;     // (nvar, nvar, nblock)
+  int wh_nm = 0;
+  std::string info;               // krige_to_str text
+
   int naug() const { return std_ck ? unbias * nvar : unbias; }
   int pdrift() const { return ndrift + naug(); }
 };
@@ -132,6 +150,15 @@ void engine_solve(Engine& e);
 // observation values of variable ivar first when it is not null.
 void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value);
 void engine_release(Engine& e);
+// weight store (kk_engine.cu): nm = largest neighbour-list length over the
+// variables; the getters copy the device store (or the staged one) into the
+// reference's column-major layouts
+int engine_weight_nm(Engine& e);
+void engine_set_weights(Engine& e, int nm, int ng, int nv, int nb, const int* nnear, const int* inear,
+                        const double* weight, const double* var);
+void engine_get_weights(Engine& e, int nm, int ng, int nv, int nb, int* nnear, int* inear, double* weight,
+                        double* var);
+void engine_free_weight_store(Engine& e);
 
 // allocator hook
 typedef void* (*alloc_fn)(size_t bytes, void* ctx);

@@ -47,6 +47,10 @@ struct SolveParams {
   int* counters;             // see KK_CNT_*
   int* fb_list;              // targets needing the generic FP64 / LDL^T path
   int* fp64_list;            // FP32 targets that need the FP64 register kernel
+  double* wout;              // kriging weights (weight store) or null: row r of target
+                             // variable jv of target t at wout[(t * nvar + jv) * wstride + r],
+                             // rows in matrix order (variable blocks, ascending index)
+  int wstride;
   double* scratch;           // generic-path workspace
   int scratch_stride;        // doubles per generic-path thread
   double refine_tol;
@@ -99,6 +103,9 @@ void launch_search_kdtree(const KkSearch& S, const int* list, const int* count, 
 size_t kd_heap_entry_bytes();
 
 void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
+// Estimates of every target from the weight store (P.wout, P.nbr, P.nnear)
+// and the current observation values (weight-store reuse).
+void launch_replay(const SolveParams& P, int nsm, cudaStream_t st);
 // Warp-per-target solve of the targets list[item0 + i], i < nitems (or
 // < *cnt - item0 when cnt is given): k_assemble writes each target's packed
 // K64 to Kg + i * N (N + 1) / 2, then k_solve_warp factors and solves; N is
@@ -112,6 +119,7 @@ void launch_factor(const SolveParams& P, int refine, int N, const int* list, con
 int solve_refine_form(const SolveParams& P, int precision);
 void launch_solve_generic(const SolveParams& P, const int* list, int list_cnt_slot, int nthreads, cudaStream_t st);
 void set_zones(cudaStream_t st);
+
 
 // Doubles of generic-kernel workspace per thread for systems of at most mtot
 // equations (neighbours + drift/unbiasedness rows) with nv right-hand sides

@@ -25,8 +25,7 @@
 #include <mutex>
 #include <string>
 
-#include "kk_device.cuh"
-#include "kk_kernels.h"
+#include "kk_solve_common.cuh"
 
 namespace kk {
 
@@ -45,45 +44,6 @@ void set_zones(cudaStream_t st) {
   }
   for (int k = 0; k < 4; ++k) z.zb[k] = hb[k];
   cudaMemcpyToSymbolAsync(c_zones, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
-}
-
-__device__ __forceinline__ double cov_pair(const SolveParams& P, int first, int second, const double* lag) {
-  if (P.st) return st_cov(P.smodels[first * P.nvar + second], P.ndim, P.tables, lag);
-  return model_cov(P.models[first * P.nvar + second], P.tables, lag);
-}
-__device__ __forceinline__ double cov0_pair(const SolveParams& P, int first, int second) {
-  if (P.st) return P.smodels[first * P.nvar + second].cov0;
-  return P.models[first * P.nvar + second].cov0;
-}
-
-// lag = (a - b) / rangescale for spatial kriging (kriging.F90:783, 905);
-// space-time lags are not scaled (kriging_st.F90:806)
-__device__ __forceinline__ void make_lag(const SolveParams& P, const double* a, const double* b, double rs,
-                                         double* lag) {
-  for (int d = 0; d < P.nlag; ++d) {
-    double t = dsub(a[d], b[d]);
-    lag[d] = P.st ? t : t / rs;
-  }
-}
-
-// F row entry a of a neighbour of variable v at observation o (obs%drift,
-// kriging_base.F90:614-624)
-__device__ __forceinline__ double f_entry(const SolveParams& P, int a, int v, int o) {
-  if (a < P.ndrift) return __ldg(&P.odrift[v][(size_t)a * P.nobs[v] + o]);
-  int ua = a - P.ndrift;
-  return P.std_ck ? (ua == v ? 1.0 : 0.0) : (ua == 0 ? 1.0 : 0.0);
-}
-// g entry a for target variable iv (block%drift, kriging_base.F90:938-951)
-__device__ __forceinline__ double g_entry(const SolveParams& P, int a, int iv, int t) {
-  if (a < P.ndrift) return P.tdrift ? __ldg(&P.tdrift[((size_t)t * P.nvar + iv) * P.ndrift + a]) : 0.0;
-  int ua = a - P.ndrift;
-  return P.std_ck ? (ua == iv ? 1.0 : 0.0) : (ua == 0 ? 1.0 : 0.0);
-}
-
-__device__ __forceinline__ void write_nan(const SolveParams& P, int t) {
-  for (int v = 0; v < P.nvar; ++v) P.est[(size_t)t * P.nvar + v] = __longlong_as_double(0x7ff8000000000000ll);
-  for (int q = 0; q < P.nvar * P.nvar; ++q)
-    P.var[(size_t)t * P.nvar * P.nvar + q] = __longlong_as_double(0x7ff8000000000000ll);
 }
 
 // ---------------------------------------------------------------------------
@@ -126,151 +86,76 @@ void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st) {
   k_bucket<<<(P.nblock + 255) / 256, 256, 0, st>>>(P, lists);
 }
 
-constexpr int MAXC = 8;  // forward-substituted columns: F + k + functionals (z, indicators)
-
-// number of functional columns carried for the estimate
-__device__ __forceinline__ int n_func(const SolveParams& P) {
-  return 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
-}
-
-// prior covariance C_ij(x0, x0) for the variance (calc_variance,
-// kriging.F90:989-1008): cov0 for points, node-pair sum for blocks.
-__device__ double base_cov(const SolveParams& P, int t, int iv, int jv) {
-  if (!P.gstart) return cov0_pair(P, iv, jv);
-  const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
-  if (k1 - k0 == 1) return cov0_pair(P, iv, jv);
-  const double c0 = cov0_pair(P, iv, jv);
-  double base = 0.0;
-  for (int i = k0; i < k1; ++i) {
-    double wi = __ldg(&P.gw[i]);
-    base = dadd(base, dmul(dmul(c0, wi), wi));
-    for (int j = i + 1; j < k1; ++j) {
-      double lag[4];
-      for (int d = 0; d < P.nlag; ++d) lag[d] = dsub(__ldg(&P.gx[d][i]), __ldg(&P.gx[d][j]));
-      base = dadd(base, dmul(dmul(dmul(cov_pair(P, iv, jv, lag), wi), __ldg(&P.gw[j])), 2.0));
+// ---------------------------------------------------------------------------
+// weight-store reuse: estimates from stored weights and neighbours
+// ---------------------------------------------------------------------------
+// load_block_weights + estimate_block_base (kriging_base.F90:2780-2797,
+// 3407-3503): est_j = sum_v sum_i z_v[inear_v(i)] w_ij, plus the Isaaks &
+// Srivastava shift (std_ck off, several variables), the simple-kriging mean
+// and the bounds.  One warp per target; the lanes take the neighbour rows
+// (weights read coalesced, values gathered), warp sums for the dot products.
+// Targets without neighbours, or marked empty or failed by the solve that
+// filled the store, give NaN.
+__global__ void __launch_bounds__(256) k_replay(const __grid_constant__ SolveParams P) {
+  const int lane = threadIdx.x & 31;
+  const int q = P.nvar;
+  const int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < P.nblock; t += nwarp) {
+    int nn[KK_MAXVAR], ist[KK_MAXVAR], npp = 0;
+#pragma unroll
+    for (int v = 0; v < KK_MAXVAR; ++v) {
+      nn[v] = v < q ? __ldg(&P.nnear[v][t]) : 0;
+      ist[v] = npp;
+      npp += nn[v];
     }
-  }
-  return base;
-}
-
-// Solve the small p x p Schur system and produce est / var from the inner
-// products G (FP64).  Column order: F (pa), k (nvar), u (nu).
-// G is symmetric, stored full C x C.
-__device__ __noinline__ void finish_outputs(const SolveParams& P, int t, const double* G, int C, const double* zmean,
-                               int* fail) {
-  const int pa = P.pa, q = P.nvar, nu = n_func(P);
-  const int kF = 0, kK = pa, kU = pa + q;
-  double S[36], lam[KK_MAXVAR][6];
-  // S = F^T K^-1 F, Cholesky (SPOTRF 'U' semantics on p x p)
-  for (int a = 0; a < pa; ++a)
-    for (int b = 0; b < pa; ++b) S[a * 6 + b] = G[(kF + a) * C + kF + b];
-  for (int j = 0; j < pa; ++j) {
-    double ajj = S[j * 6 + j];
-    for (int k = 0; k < j; ++k) ajj -= S[k * 6 + j] * S[k * 6 + j];
-    if (!(ajj > 0.0)) { *fail = 1; return; }
-    ajj = sqrt(ajj);
-    S[j * 6 + j] = ajj;
-    for (int i = j + 1; i < pa; ++i) {
-      double s = S[j * 6 + i];
-      for (int k = 0; k < j; ++k) s -= S[k * 6 + j] * S[k * 6 + i];
-      S[j * 6 + i] = s / ajj;
+    if (npp == 0 || (__ldg(&P.status[t]) & (KK_ST_EMPTY | KK_ST_FAIL))) {
+      if (lane == 0)
+        for (int v = 0; v < q; ++v) P.est[(size_t)t * q + v] = __longlong_as_double(0x7ff8000000000000ll);
+      continue;
     }
-  }
-  for (int iv = 0; iv < q; ++iv) {
-    // rhs_small = F^T K^-1 k - g  (solver.f90:282-286)
-    double r[6];
-    for (int a = 0; a < pa; ++a) r[a] = G[(kF + a) * C + kK + iv] - g_entry(P, a, iv, t);
-    for (int i = 0; i < pa; ++i) {  // U^T y = r
-      double s = r[i];
-      for (int k = 0; k < i; ++k) s -= S[k * 6 + i] * r[k];
-      r[i] = s / S[i * 6 + i];
-    }
-    for (int i = pa - 1; i >= 0; --i) {  // U x = y
-      double s = r[i];
-      for (int k = i + 1; k < pa; ++k) s -= S[i * 6 + k] * r[k];
-      r[i] = s / S[i * 6 + i];
-    }
-    for (int a = 0; a < pa; ++a) lam[iv][a] = r[a];
-  }
-  // estimate (estimate_block_base, kriging_base.F90:3424-3468)
-  for (int jv = 0; jv < q; ++jv) {
-    // z^T w = z^T K^-1 k - (z^T K^-1 F) lambda
-    double avg = G[kU * C + kK + jv];
-    for (int a = 0; a < pa; ++a) avg -= G[kU * C + kF + a] * lam[jv][a];
-    if (nu > 1) {
-      double tw[KK_MAXVAR], tws = 0.0;
+    double tmean[KK_MAXVAR];
+    if (P.ck_isa) {
       for (int v = 0; v < q; ++v) {
-        tw[v] = G[(kU + 1 + v) * C + kK + jv];
-        for (int a = 0; a < pa; ++a) tw[v] -= G[(kU + 1 + v) * C + kF + a] * lam[jv][a];
-        tws += tw[v];
+        double sz = 0.0;
+        for (int i = lane; i < nn[v]; i += 32)
+          sz += __ldg(&P.oval[v][__ldg(&P.nbr[v][(size_t)t * P.mmax[v] + i])]);
+        sz = warp_sum(sz);
+        tmean[v] = nn[v] > 0 ? sz / nn[v] : 0.0;
       }
-      if (P.ck_isa)
-        for (int v = 0; v < q; ++v)
-          if (v != jv && zmean[KK_MAXVAR + v] > 0.0) avg += (zmean[jv] - zmean[v]) * tw[v];
+    }
+    for (int jv = 0; jv < q; ++jv) {
+      const double* w = P.wout + ((size_t)t * q + jv) * P.wstride;
+      double avg = 0.0, tws = 0.0;
+      for (int v = 0; v < q; ++v) {
+        double dot = 0.0, sw = 0.0;
+        for (int i = lane; i < nn[v]; i += 32) {
+          const double wt = __ldg(&w[ist[v] + i]);
+          dot = fma(__ldg(&P.oval[v][__ldg(&P.nbr[v][(size_t)t * P.mmax[v] + i])]), wt, dot);
+          sw += wt;
+        }
+        dot = warp_sum(dot);
+        sw = warp_sum(sw);
+        avg += dot;
+        tws += sw;
+        if (P.ck_isa && v != jv && nn[v] > 0) avg += (tmean[jv] - tmean[v]) * sw;
+      }
       if (P.unbias == 0 && P.sk_mean[jv] != 0.0) avg += (1.0 - tws) * P.sk_mean[jv];
-    }
-    if (avg < P.bounds[0]) avg = P.bounds[0];
-    if (avg > P.bounds[1]) avg = P.bounds[1];
-    P.est[(size_t)t * q + jv] = avg;
-  }
-  // variance: base - (w_iv^T k_jv + lambda_iv^T g_jv) (calc_variance)
-  double* V = P.var + (size_t)t * q * q;
-  for (int iv = 0; iv < q; ++iv)
-    for (int jv = iv; jv < q; ++jv) {
-      double d = G[(kK + iv) * C + kK + jv];
-      for (int a = 0; a < pa; ++a) d -= lam[iv][a] * G[(kF + a) * C + kK + jv];
-      for (int a = 0; a < pa; ++a) d += lam[iv][a] * g_entry(P, a, jv, t);
-      double v = base_cov(P, t, iv, jv) - d;
-      V[iv + jv * q] = v;
-      V[jv + iv * q] = v;
-    }
-  for (int iv = 0; iv < q; ++iv) {
-    double d = V[iv + iv * q];
-    if (d < 0.0) V[iv + iv * q] = 0.0;
-    for (int jv = iv + 1; jv < q; ++jv) {
-      double o = V[jv + iv * q];
-      if (o < 0.0) o = 0.0;
-      V[jv + iv * q] = o;
-      V[iv + jv * q] = o;
+      if (avg < P.bounds[0]) avg = P.bounds[0];
+      if (avg > P.bounds[1]) avg = P.bounds[1];
+      if (lane == 0) P.est[(size_t)t * q + jv] = avg;
     }
   }
 }
 
-// Covariance of one neighbour row (coordinates xr, variable vr) with the
-// target for target variable iv, averaged over block nodes (assemble_rhs,
-// kriging.F90:889-910); defined after the fast covariance paths.
-__device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const double* xr, int vr, int iv, double rs);
+void launch_replay(const SolveParams& P, int nsm, cudaStream_t st) {
+  const int need = (P.nblock + 7) / 8;  // eight warps per block
+  const int blocks = std::max(1, std::min(need, nsm * 8));
+  k_replay<<<blocks, 256, 0, st>>>(P);
+}
 
 }  // namespace kk
 
 #include "kk_warp.cuh"
-
-namespace kk {
-
-// rhs_cov_row: the space-time fast path serves block nodes too
-__device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, const double* xr, int vr, int iv, double rs) {
-  double tmp = 0.0;
-  if (P.gstart) {
-    const int k0 = __ldg(&P.gstart[t]), k1 = __ldg(&P.gstart[t + 1]);
-    for (int k = k0; k < k1; ++k) {
-      double node[4], lag[4];
-      for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
-      make_lag(P, xr, node, rs, lag);
-      const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
-      tmp = dadd(tmp, dmul(cv, __ldg(&P.gw[k])));
-    }
-  } else {
-    double node[4], lag[4];
-    for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
-    make_lag(P, xr, node, rs, lag);
-    const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
-    tmp = dadd(tmp, dmul(cv, 1.0));
-  }
-  return tmp;
-}
-
-}  // namespace kk
-
 
 namespace kk {
 
@@ -585,8 +470,15 @@ __global__ void k_solve_generic(SolveParams P, const int* __restrict__ list, con
       atomicAdd(&P.counters[KK_CNT_FAIL], 1);
       P.status[t] |= KK_ST_FAIL;
       write_nan(P, t);
+      if (P.wout)  // the reference's failed system keeps NaN weights
+        for (int c = 0; c < q; ++c)
+          for (int k = 0; k < npp; ++k)
+            P.wout[((size_t)t * q + c) * P.wstride + k] = __longlong_as_double(0x7ff8000000000000ll);
       continue;
     }
+    if (P.wout)  // kriging weights of the neighbour rows (assign_weight_ctx)
+      for (int c = 0; c < q; ++c)
+        for (int k = 0; k < npp; ++k) P.wout[((size_t)t * q + c) * P.wstride + k] = X[c + (size_t)k * q];
     // calc_variance + estimate_block_base
     double* Vt = P.var + (size_t)t * q * q;
     for (int iv = 0; iv < q; ++iv)
@@ -637,26 +529,27 @@ __global__ void k_solve_generic(SolveParams P, const int* __restrict__ list, con
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <typename T, int N, bool REFINE, int CB>
+template <typename T, int N, bool REFINE, int CB, bool WT = false>
 static void launch_warp(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
                         const double* Kg, int slot, int nsm, cudaStream_t st) {
   constexpr int WPC = warp_cta<T, N, REFINE>();
-  const size_t smem = sizeof(WarpSmem<T, N, REFINE, CB>) * WPC;
+  const size_t smem = sizeof(WarpSmem<T, N, REFINE, CB, WT>) * WPC;
   // per instantiation and device: function attributes belong to a context
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_solve_warp<T, N, REFINE, CB, WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE, CB>, 32 * WPC, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_warp<T, N, REFINE, CB, WT>, 32 * WPC, smem);
   if (occ < 1) occ = 1;
   int blocks = nsm * occ;
   const int need = (nitems + WPC - 1) / WPC;
   if (need < blocks) blocks = need > 0 ? need : 1;
-  k_solve_warp<T, N, REFINE, CB><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
+  k_solve_warp<T, N, REFINE, CB, WT><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
 }
 
 int solve_refine_form(const SolveParams& P, int precision) {
@@ -700,6 +593,15 @@ void launch_factor(const SolveParams& P, int refine, int N, const int* list, con
       if (narrow) launch_warp<float, 64, true, 3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
       else if (C <= 5) launch_warp<float, 64, true, 5>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
       else launch_warp<float, 64, true, KK_REFINE_COLS>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    }
+  } else if (P.wout) {
+    // FP64 form with the kriging weights of every target (weight store)
+    if (N == 32) {
+      if (narrow) launch_warp<double, 32, false, 3, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<double, 32, false, MAXC, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    } else {
+      if (narrow) launch_warp<double, 64, false, 3, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+      else launch_warp<double, 64, false, MAXC, true>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
     }
   } else {
     if (N == 32) {

@@ -30,161 +30,9 @@
 //      the same inner products are taken against the refined W.
 #pragma once
 
-// right-hand-side columns carried by the refinement form (F | k | u); systems
-// with more columns are solved by the FP64 form
-#define KK_REFINE_COLS 6
-
 namespace kk {
 
-__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
-
-// zone constants of the lookup tables, held in registers
-struct ZoneRegs {
-  double zb1, zb2, zb3, i0, i1, i2;
-  int o1, o2, n0, n1, n2;
-};
-
-__device__ __forceinline__ ZoneRegs load_zones() {
-  ZoneRegs z;
-  z.zb1 = c_zones.zb[1];
-  z.zb2 = c_zones.zb[2];
-  z.zb3 = c_zones.zb[3];
-  z.i0 = c_zones.inv_dh[0];
-  z.i1 = c_zones.inv_dh[1];
-  z.i2 = c_zones.inv_dh[2];
-  z.o1 = c_zones.off[1];
-  z.o2 = c_zones.off[2];
-  z.n0 = c_zones.zn[0];
-  z.n1 = c_zones.zn[1];
-  z.n2 = c_zones.zn[2];
-  return z;
-}
-
-// tab_lookup without divergent constant-memory indexing: the same zone
-// choice, index and interpolation (variogram.f90:353-382, 682-710) from
-// register selects.  Valid for 0 <= h < zb3.
-__device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, const ZoneRegs& z, double h) {
-  const bool z0 = h < z.zb1, z1 = h < z.zb2;
-  const double lo = z0 ? 0.0 : (z1 ? z.zb1 : z.zb2);
-  const double inv = z0 ? z.i0 : (z1 ? z.i1 : z.i2);
-  const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
-  const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
-  double fi = dmul(dsub(h, lo), inv);
-  const int ii = (int)fi;
-  const int i = off + min(ii, nm1);
-  fi = dsub(fi, (double)ii);
-  const double2 t = __ldg(&tab[i]);
-  return dadd(t.x, dmul(fi, t.y));
-}
-
-// analytic tail past the last table zone (struct_cov_h), kept out of line so
-// that the rarely taken shape code does not raise the kernels' register count
-__device__ __noinline__ double tail_cov(const KkModel* m, double h) { return model_cov_h(*m, h); }
-
-// COV(vgm(first, second), lag) for models without the fast path; the lag
-// travels by value so that callers keep it in registers
-__device__ __noinline__ double cov_pair_call(const SolveParams& P, int first, int second, double l0, double l1,
-                                             double l2, double l3) {
-  const double lag[4] = {l0, l1, l2, l3};
-  return cov_pair(P, first, second, lag);
-}
-
-// h = |M lag| with fused multiply-adds and h = h2 * rsqrt(h2): within a few
-// ulp of aniso_h, which moves the interpolated covariance by far less than
-// the solve tolerance (the table is continuous in h)
-__device__ __forceinline__ double aniso_h_fast(const double* m, int ndim, const double* lag) {
-  double h2;
-  if (ndim == 2) {
-    const double rx = fma(m[0], lag[0], m[3] * lag[1]);
-    const double ry = fma(m[1], lag[0], m[4] * lag[1]);
-    h2 = fma(rx, rx, ry * ry);
-  } else if (ndim == 3) {
-    const double rx = fma(m[0], lag[0], fma(m[3], lag[1], m[6] * lag[2]));
-    const double ry = fma(m[1], lag[0], fma(m[4], lag[1], m[7] * lag[2]));
-    const double rz = fma(m[2], lag[0], fma(m[5], lag[1], m[8] * lag[2]));
-    h2 = fma(rx, rx, fma(ry, ry, rz * rz));
-  } else {
-    return fabs(m[0] * lag[0]);
-  }
-  return h2 > 0.0 ? h2 * rsqrt(h2) : 0.0;
-}
-
-// The single model of single-variable spatial kriging (P.fast_model); its
-// transform and table offsets travel in the kernel parameters, which the
-// kernels read as constant operands instead of holding registers.
-// Level B (1): COV(vgm, lag) = table(aniso_h(bmat, lag)), analytic tail past
-// the table.
-// Level A (2): COV(vgm, lag) = sum over the structures s of
-// table_s(k_s * |fm lag|), in structure order like the general model_cov.
-__device__ __noinline__ double tail_comp(const KkComp* c, double h) { return comp_cov_h(*c, h); }
-template <int FM>  // 1 or 2 when known at compile time, 0: read P.fast_model
-__device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag) {
-  const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
-  if (FM == 1 || (FM == 0 && P.fast_model == 1)) {
-    if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off, z, h);
-    return P.fm_tail ? tail_cov(P.models, h) : 0.0;
-  }
-  double res = 0.0;
-#pragma unroll
-  for (int s = 0; s < KK_FA_MAXS; ++s) {
-    if (s < P.fa_nst) {
-      const double hs = P.fa_k[s] * h;
-      double g;
-      if (hs < z.zb3) g = tab_fast(P.tables + P.fa_off[s], z, hs);
-      else g = ((P.fa_tailmask >> s) & 1) ? tail_comp(&P.models[0].comp[s], hs) : 0.0;
-      res = dadd(res, g);
-    }
-  }
-  return res;
-}
-
-// Space-time (P.fast_model == 4): st_cov of one variable from the spatial
-// table at |fm lag_s| and the temporal table at |ft_k dt| (dt = lag[P.ndim]),
-// combined in st_cov's order.
-__device__ __forceinline__ double fast_cov_st(const SolveParams& P, const ZoneRegs& z, const double* lag) {
-  const double hs = aniso_h_fast(P.fm, P.fm_ndim, lag);
-  const double dt = P.ndim == 1 ? lag[1] : (P.ndim == 2 ? lag[2] : lag[3]);
-  const double ht = fabs(P.ft_k * fabs(dt));
-  double cs, ct;
-  if (hs < z.zb3) cs = tab_fast(P.tables + P.fm_tab_off, z, hs);
-  else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
-  if (ht < z.zb3) ct = tab_fast(P.tables + P.ft_off, z, ht);
-  else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
-  if (P.st_kind == 1) return dadd(dadd(dmul(dmul(P.st_kps, cs), ct), cs), ct);
-  return dadd(cs, ct);
-}
-
-// Two variables (P.fast_model == 3): COV(vgm(i, j), lag) at pair = 2 i + j from
-// that pair's Level-B table, its Level-A tables, or its analytic structures
-// (vgm(i, j), i > j, as the general model_cov evaluates it), every structure
-// at h_s = k_s * |fm lag|.
-__device__ __forceinline__ double fast_cov_pair(const SolveParams& P, const ZoneRegs& z, const double* lag,
-                                                int pair) {
-  const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
-  const int kind = P.fq_kind[pair];
-  if (kind == 1) {
-    const double hs = P.fq_k[pair][0] * h;
-    if (hs < z.zb3) return tab_fast(P.tables + P.fq_off[pair][0], z, hs);
-    return (P.fq_tail[pair] & 1) ? tail_cov(P.models + pair, hs) : 0.0;
-  }
-  double res = 0.0;
-  const int nst = P.fq_nst[pair];
-#pragma unroll
-  for (int s = 0; s < KK_FA_MAXS; ++s) {
-    if (s < nst) {
-      const double hs = P.fq_k[pair][s] * h;
-      double g;
-      if (kind == 3) g = comp_cov_h(P.models[pair].comp[s], hs);
-      else if (hs < z.zb3) g = tab_fast(P.tables + P.fq_off[pair][s], z, hs);
-      else g = ((P.fq_tail[pair] >> s) & 1) ? tail_comp(&P.models[pair].comp[s], hs) : 0.0;
-      res = dadd(res, g);
-    }
-  }
-  return res;
-}
-
-template <typename T, int N, bool REFINE, int CB>
+template <typename T, int N, bool REFINE, int CB, bool WT = false>
 struct __align__(16) WarpSmem {
   double x[4][N];          // neighbour coordinates (nlag)
   double z[N];             // neighbour values
@@ -197,22 +45,12 @@ struct __align__(16) WarpSmem {
   float L[REFINE ? N * (N - 1) / 2 : 1];   // FP32 factor, strictly lower, packed by column
   float invd[REFINE ? N : 1];              // 1 / L[j][j]
   double W[REFINE ? CB * N : 1];           // current solution, broadcast for the residual
+  // weight store (WT): strictly lower L packed by column after one leading
+  // zero entry (L[r][j] at lcol(j) - j + r), 1 / L[j][j], Lagrange multipliers
+  double Lw[WT ? N * (N - 1) / 2 + 2 : 1];
+  double invw[WT ? N : 1];
+  double lam[WT ? KK_MAXVAR * 6 : 1];
 };
-
-// start of column c of the strictly-lower packed factor
-template <int N>
-__device__ __forceinline__ int lcol(int c) { return c * (N - 1) - (c * (c - 1)) / 2; }
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
 
 // Triangular sweeps of the refinement form over a lane's right-hand-side
 // rows r = 32 m + 4 pc + pr, with L (strictly lower, packed by column) and
@@ -270,38 +108,6 @@ __device__ __forceinline__ void sweep_fwd(T (&v)[RM][CB], const float* __restric
   }
 }
 
-// Neighbour rows of target t in matrix order (variable blocks in order,
-// ascending index within a block: assemble_linear_system_base,
-// kriging_base.F90:3159-3235) into per-warp shared arrays.  Returns the row
-// count n and the block starts of variables 1..3.
-template <int N>
-__device__ __forceinline__ int gather_rows(const SolveParams& P, int t, int lane, double (*x)[N], double* z,
-                                           int* obs, int* var, int& ist1, int& ist2, int& ist3) {
-  const int q = P.nvar;
-  int n = 0;
-  ist1 = ist2 = ist3 = 0x7fffffff;
-#pragma unroll
-  for (int v = 0; v < KK_MAXVAR; ++v) {
-    if (v < q) {
-      if (v == 1) ist1 = n;
-      if (v == 2) ist2 = n;
-      if (v == 3) ist3 = n;
-      n += __ldg(&P.nnear[v][t]);
-    }
-  }
-  for (int r = lane; r < n; r += 32) {
-    const int v = (r >= ist1) + (r >= ist2) + (r >= ist3);
-    const int i0 = v == 0 ? 0 : (v == 1 ? ist1 : (v == 2 ? ist2 : ist3));
-    const int o = __ldg(&P.nbr[v][(size_t)t * P.mmax[v] + (r - i0)]);
-    obs[r] = o;
-    var[r] = v;
-    for (int d = 0; d < P.nlag; ++d) x[d][r] = __ldg(&P.ox[v][d][o]);
-    if (z) z[r] = __ldg(&P.oval[v][o]);
-  }
-  __syncwarp();
-  return n;
-}
-
 // Covariance matrix K (assemble_lhs, kriging.F90:714-849; lag = x_c - x_r,
 // diagonal cov0 + observation variance + local nugget) of the targets
 // list[item0 + i], i < count, written packed row-major lower to
@@ -309,7 +115,12 @@ __device__ __forceinline__ int gather_rows(const SolveParams& P, int t, int lane
 // spread evenly over the lanes (stores are contiguous across the warp).
 // This is the part of the solve that is bound by covariance-table latency,
 // so it runs as its own kernel with many resident warps; the factorisation
-// kernel then reads K from this buffer (L2-resident in chunks).
+// kernel then reads K from this buffer.  On the fast covariance paths an
+// entry follows the reference's table lookup (zones, index, linear
+// interpolation) at the distance |u_c - u_r| of target-centred transformed
+// coordinates, with its square root from an FP32 seed and one FP64 Newton
+// step: a few ulp from the reference's arithmetic, which moves the solution
+// by about the condition number times 1e-15.
 template <int N, int FM>
 __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ SolveParams P,
                                                      const int* __restrict__ list,
@@ -318,15 +129,30 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
   constexpr int NK = N * (N + 1) / 2;
   struct Rows {
     double x[4][N];
+    double u[3][N];  // target-centred transformed coordinates (fast paths)
     int obs[N];
     int var[N];
   };
   __shared__ Rows rows[8];
+  __shared__ PairModel s_pm[4];  // two-variable fast path (FM 3), dynamic pair index
+  if (FM == 3 && threadIdx.x < 4) {
+    PairModel& m = s_pm[threadIdx.x];
+    m.kind = P.fq_kind[threadIdx.x];
+    m.nst = P.fq_nst[threadIdx.x];
+    m.tail = P.fq_tail[threadIdx.x];
+    for (int q2 = 0; q2 < KK_FA_MAXS; ++q2) {
+      m.off[q2] = P.fq_off[threadIdx.x][q2];
+      m.k[q2] = P.fq_k[threadIdx.x][q2];
+    }
+  }
+  __syncthreads();
   Rows& s = rows[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   int count = nitems;
   if (list_count) count = min(nitems, *list_count - item0);
   const bool fast = P.fast_model != 0;
+  const int fd = P.fm_ndim;                       // transformed dimensions
+  const int nsp = FM == 4 ? P.nlag - 1 : P.nlag;  // spatial coordinates
   const ZoneRegs zr = load_zones();
   const int nwarp = gridDim.x * (blockDim.x >> 5);
   for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < count; it += nwarp) {
@@ -336,6 +162,28 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
     const double rs = P.rs ? __ldg(&P.rs[t]) : 1.0;
     const double ln = P.ln ? __ldg(&P.ln[t]) : 0.0;
     const bool scale_lag = !P.st && rs != 1.0;  // warp-uniform
+    if (fast) {
+      // u = M (x - x_t) / rangescale: the anisotropic distance of a pair is
+      // |u_c - u_r|, one transform per neighbour instead of one per pair
+      double xt[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d < nsp) xt[d] = __ldg(&P.tx[d][t]);
+      for (int r = lane; r < n; r += 32) {
+        double l[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          if (d < nsp) {
+            l[d] = s.x[d][r] - xt[d];
+            if (scale_lag) l[d] = l[d] / rs;
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (d < fd) s.u[d][r] = fma(P.fm[d], l[0], fma(P.fm[3 + d], l[1], P.fm[6 + d] * l[2]));
+      }
+      __syncwarp();
+    }
     double* K = Kg + (size_t)it * NK;
     const int E = n * (n + 1) / 2;
     int r = 0, c = lane;
@@ -345,6 +193,20 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
       double kv;
       if (c == r) {
         kv = dadd(dadd(cov0_pair(P, vr, vr), __ldg(&P.ovar[vr][s.obs[r]])), ln);
+      } else if (fast) {
+        const double d0 = s.u[0][c] - s.u[0][r];
+        double h2 = d0 * d0;
+        if (fd > 1) {
+          const double d1 = s.u[1][c] - s.u[1][r];
+          h2 = fma(d1, d1, h2);
+        }
+        if (fd > 2) {
+          const double d2 = s.u[2][c] - s.u[2][r];
+          h2 = fma(d2, d2, h2);
+        }
+        const double hh = fd == 1 ? fabs(d0) : sqrt_newton(h2);
+        kv = FM == 4 ? cov_st_h(P, zr, hh, s.x[nsp][c] - s.x[nsp][r])
+                     : cov_h<FM == 4 ? 1 : FM>(P, zr, hh, s_pm, FM == 3 ? vr * 2 + s.var[c] : 0);
       } else {
         double lag[4];
 #pragma unroll
@@ -353,10 +215,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
 #pragma unroll
           for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
         }
-        kv = fast ? (FM == 3   ? fast_cov_pair(P, zr, lag, vr * 2 + s.var[c])
-                     : FM == 4 ? fast_cov_st(P, zr, lag)
-                               : fast_cov<FM>(P, zr, lag))
-                  : cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
+        kv = cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
       }
       K[e] = kv;
       c += 32;
@@ -382,12 +241,15 @@ constexpr int warp_min_ctas() { return N == 64 ? (REFINE ? (CB == 3 ? 4 : 3) : 1
 // CB: right-hand-side columns held per row at compile time (F | k | u);
 // 3 covers ordinary and simple kriging of one variable, the wider forms
 // cover drift and cokriging.
-template <typename T, int N, bool REFINE, int CB>
+// WT (FP64 form only): also the kriging weights of every target, for the
+// weight store (P.wout)
+template <typename T, int N, bool REFINE, int CB, bool WT = false>
 __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T, N, REFINE, CB>())
     k_solve_warp(const __grid_constant__ SolveParams P, const int* __restrict__ list,
                  const int* __restrict__ list_count, int item0, int nitems, const double* __restrict__ Kg,
                  int work_slot) {
-  using WS = WarpSmem<T, N, REFINE, CB>;
+  static_assert(!(WT && REFINE), "the weight store is filled by the FP64 form");
+  using WS = WarpSmem<T, N, REFINE, CB, WT>;
   constexpr int RI = N / 4, CI = N / 8, RM = N / 32;
   // column-buffer row stride: padded so the four row classes fall in
   // different banks and stay 16-byte aligned
@@ -408,6 +270,9 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
 
 
   int n_chol = 0, n_iter = 0;
+  if constexpr (WT) {
+    if (lane == 0) s.Lw[0] = 0.0;
+  }
   for (;;) {
     int item = 0;
     if (lane == 0) item = atomicAdd(&P.counters[work_slot], 1);
@@ -512,6 +377,9 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
         if constexpr (REFINE) {
           if (lane == 0) s.invd[j] = (float)inv;
         }
+        if constexpr (WT) {
+          if (lane == 0) s.invw[j] = (double)inv;
+        }
         if (pc == jj) {
 #pragma unroll
           for (int ri = 2 * jb; ri < RI; ++ri) {
@@ -519,6 +387,9 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
             const T l = (r > j) ? a[ri][jb] * inv : T(0);
             if (REFINE) a[ri][jb] = l;
             cw[pr * RIP + ri] = l;
+            if constexpr (WT) {
+              if (r > j) s.Lw[lcol<N>(j) - j + r] = (double)l;
+            }
           }
         }
         const int owner = ((j >> 2) & 7) * 4 + (j & 3);
@@ -689,9 +560,9 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
       }
     }
     __syncwarp();
+    int f = 0;
     if (lane == 0) {
-      int f = 0;
-      finish_outputs(P, t, s.G, C, s.zmean, &f);
+      finish_outputs(P, t, s.G, C, s.zmean, &f, WT ? s.lam : nullptr);
       if (f) {
         P.status[t] |= KK_ST_LDLT;
         const int p = atomicAdd(&P.counters[KK_CNT_FB], 1);
@@ -701,6 +572,47 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
       }
     }
     __syncwarp();
+    if constexpr (WT) {
+      // kriging weights w = K^-1 (k - F lambda) = L^-T (y_k - Y_F lambda)
+      // (assign_weight_ctx, kriging_base.F90:2428-2439): back sweep on the
+      // unit-diagonal factor, rows scaled by 1 / L[r][r] at the end; a target
+      // sent to the general kernel gets its weights there
+      f = __shfl_sync(FULL, f, 0);
+      if (!f) {
+        int lrow[RM];
+#pragma unroll
+        for (int m = 0; m < RM; ++m) lrow[m] = lcol<N>(32 * m + lane) - (32 * m + lane);
+        for (int jv = 0; jv < q; ++jv) {
+          double v[RM];
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            double vm = 0.0;
+#pragma unroll
+            for (int k = 0; k < CB; ++k)
+              if (k == pa + jv) vm = (double)b[m][k];
+#pragma unroll
+            for (int k = 0; k < CB; ++k)
+              if (k < pa) vm = fma(-(double)b[m][k], s.lam[jv * 6 + k], vm);
+            v[m] = vm;
+          }
+          for (int j = n - 1; j >= 0; --j) {
+            const double mine = (RM > 1 && (j >> 5) == 1) ? v[RM - 1] : v[0];
+            const double nx = -__shfl_sync(FULL, mine, j & 31) * s.invw[j];
+#pragma unroll
+            for (int m = 0; m < RM; ++m) {
+              const int r = 32 * m + lane;
+              v[m] = fma(s.Lw[r < j ? lrow[m] + j : 0], nx, v[m]);
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < RM; ++m) {
+            const int r = 32 * m + lane;
+            if (r < n) P.wout[((size_t)t * q + jv) * P.wstride + r] = v[m] * s.invw[r];
+          }
+        }
+      }
+      __syncwarp();
+    }
   }
   if (lane == 0) {
     if (n_chol) atomicAdd(&P.counters[KK_CNT_CHOL], n_chol);

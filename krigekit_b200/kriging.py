@@ -83,6 +83,8 @@ class Kriging:
         nmin: int = 0,
         device: Optional[int] = None,
     ):
+        if store_weight and use_old_weight:
+            raise ValueError("store_weight and use_old_weight are mutually exclusive")
         lib = _lib.load()
         import torch
         if not torch.cuda.is_available():
@@ -119,6 +121,8 @@ class Kriging:
         self.seed = seed
         self.precision = precision
         self.device = dev
+        self.store_weight = store_weight
+        self.use_old_weight = use_old_weight
         self._nblock = 0
         self._nobs = np.zeros(nvar, dtype=np.int64)
         self._nvgm_struct = np.zeros((nvar, nvar), dtype=np.int64)
@@ -358,6 +362,91 @@ class Kriging:
     def get_result_df(self):
         import pandas as pd
         return pd.DataFrame(self.get_result_array())
+
+    def get_variance_all(self, copy: bool = False):
+        """Conditional covariance matrix of all variables, (nblock, nvar, nvar) (kriging.py:1714-1735)."""
+        nb, nv = self._nb(), self.nvar
+        out = _fempty((nb, nv, nv))
+        _lib.call("krige_get_variance_all", self._h(), nb, nv, _dptr(out))
+        return np.array(out, order="C", copy=True) if copy else out
+
+    # ------------------------------------------------------------ weight store
+    def free_weight_store(self):
+        """Release the in-memory weight store (kriging.py:1746-1749)."""
+        _lib.call("krige_free_weight_store", self._h())
+
+    def get_weights(self) -> dict:
+        """Stored kriging weights and neighbours (kriging.py:1875-1971).
+
+        Keys ``nnear`` (nblock, ngroups), ``inear`` (nblock, ngroups, nmax,
+        1-based, zero-padded), ``weight`` (nblock, nvar, ngroups, nmax) --
+        (nblock, ngroups, nmax) for one variable -- and ``variance`` ((nblock,)
+        or (nblock, nvar, nvar)).  Needs ``store_weight=True`` and a solve.
+        """
+        nm, ng, nb = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _lib.call("krige_get_weight_dims", self._h(), ctypes.byref(nm), ctypes.byref(ng), ctypes.byref(nb))
+        nm, ng, nb, nv = nm.value, ng.value, nb.value, self.nvar
+        nnear_f = np.zeros((ng, nb), dtype=np.int32, order="F")
+        inear_f = np.zeros((nm, ng, nb), dtype=np.int32, order="F")
+        weight_f = np.zeros((nm, ng, nv, nb), dtype=np.float64, order="F")
+        var_f = np.zeros((nv, nv, nb), dtype=np.float64, order="F")
+        _lib.call("krige_get_weight_nnear", self._h(), ng, nb, _iptr(nnear_f))
+        _lib.call("krige_get_weight_inear", self._h(), nm, ng, nb, _iptr(inear_f))
+        _lib.call("krige_get_weight_data", self._h(), nm, ng, nv, nb, _dptr(weight_f))
+        _lib.call("krige_get_weight_var", self._h(), nv, nb, _dptr(var_f))
+        weight = np.ascontiguousarray(weight_f.T)  # (nb, nv, ng, nm)
+        var = np.ascontiguousarray(var_f.T)        # (nb, nv, nv)
+        if nv == 1:
+            weight = weight[:, 0, :, :]
+            var = var[:, 0, 0]
+        return {"nnear": np.ascontiguousarray(nnear_f.T), "inear": np.ascontiguousarray(inear_f.T),
+                "weight": weight, "variance": var}
+
+    def set_weights(self, weights: dict) -> None:
+        """Load a weight store so that solve() re-estimates from it (kriging.py:1752-1873)."""
+        if self.store_weight:
+            raise ValueError("set_weights() is incompatible with store_weight=True. "
+                             "Construct Kriging without store_weight=True when reusing weights.")
+        nnear = np.ascontiguousarray(weights["nnear"], dtype=np.int32)
+        inear = np.ascontiguousarray(weights["inear"], dtype=np.int32)
+        weight = np.asarray(weights["weight"], dtype=np.float64)
+        if nnear.ndim != 2:
+            raise ValueError("nnear must be 2-D (nblock, ngroups)")
+        if inear.ndim != 3:
+            raise ValueError("inear must be 3-D (nblock, ngroups, nmax)")
+        nb, ng = nnear.shape
+        nm = inear.shape[2]
+        nv = self.nvar
+        if weight.ndim == 3:
+            weight_f = np.asfortranarray(weight.T[:, :, np.newaxis, :])
+        elif weight.ndim == 4:
+            weight_f = np.asfortranarray(np.transpose(weight, (3, 2, 1, 0)))
+        else:
+            raise ValueError("weight must be 3-D (nblock, ngroups, nmax) or 4-D (nblock, nvar, ngroups, nmax)")
+        var = weights.get("variance")
+        if var is not None:
+            var = np.asarray(var, dtype=np.float64)
+            if var.ndim == 1:
+                var = var[:, np.newaxis, np.newaxis]
+            var_f = np.asfortranarray(np.transpose(var, (1, 2, 0)))
+        else:
+            var_f = np.zeros((nv, nv, nb), dtype=np.float64, order="F")
+        order = np.ascontiguousarray(np.arange(1, nb + 1, dtype=np.int32))
+        nnear_f = np.asfortranarray(nnear.T)
+        inear_f = np.asfortranarray(inear.T)
+        _lib.call("krige_set_weights", self._h(), nm, ng, nv, nb, _iptr(nnear_f), _iptr(inear_f),
+                  _dptr(weight_f), _iptr(order), _dptr(var_f))
+        self.use_old_weight = True
+
+    def get_info(self) -> str:
+        """Configuration summary (kriging.py:1973-1977)."""
+        ptr = self._lib.krige_to_str(self._h())
+        if not ptr:
+            return ""
+        return ctypes.cast(ptr, ctypes.c_char_p).value.decode("utf-8", errors="ignore")
+
+    def __str__(self):
+        return self.get_info()
 
     # ------------------------------------------------------------ extensions
     def get_neighbours(self, ivar: int = 1):

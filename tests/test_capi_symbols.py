@@ -19,7 +19,7 @@ def _declared():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"\b(?:int|void)\s+(krige_\w+)\s*\(", src):
+        for m in re.finditer(r"\b(?:int|void|char)\s*\**\s*(krige_\w+)\s*\(", src):
             names.add(m.group(1))
     return sorted(names)
 
