@@ -24,6 +24,13 @@ extern "C" {
 
 /* kriging_capi.F90:43-57 krige_create: new handle (1-based registry slot). */
 int krige_create(int64_t *handle);
+/* kriging_capi.F90:83-100 krige_ind_create: handle for multiple indicator kriging; after
+ * each solve the first ncat estimates per target (category probabilities) are clipped to
+ * [0, 1] and normalised to sum to one (post_solve_indicator, kriging_indicator.F90:170-185). */
+int krige_ind_create(int64_t *handle);
+/* kriging_capi.F90:113- krige_ind_set_ncat: categories (1..nvar), after krige_initialize;
+ * variables past ncat are secondary co-variates outside the normalisation. */
+int krige_ind_set_ncat(int64_t handle, int ncat);
 /* kriging_capi_common.F90 krige_destroy (release_obj_base): frees device and host state. */
 int krige_destroy(int64_t *handle);
 

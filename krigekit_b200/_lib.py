@@ -29,6 +29,8 @@ FREE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p)
 SIGNATURES = {
     "krige_create": ([_p_i64], _c_int),
     "krige_destroy": ([_p_i64], _c_int),
+    "krige_ind_create": ([_p_i64], _c_int),
+    "krige_ind_set_ncat": ([_c_i64, _c_int], _c_int),
     "krige_initialize": ([_c_i64, _c_int, _c_int, _c_int, _c_int, _c_int,
                           _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
                           _c_int, _c_char_p, _p_dbl, _c_int], _c_int),

@@ -122,6 +122,29 @@ int krige_create(int64_t* handle) {
   KK_GUARD_END
 }
 
+// krige_ind_create, kriging_capi.F90:83-100: a handle whose solves end with
+// the indicator post-processing (category probabilities clipped to [0, 1]
+// and normalised, post_solve_indicator, kriging_indicator.F90:170-185)
+int krige_ind_create(int64_t* handle) {
+  if (krige_create(handle) != 0) return 1;
+  Engine* e = get(*handle);
+  if (!e) return 1;
+  e->indicator = 1;
+  return 0;
+}
+
+// krige_ind_set_ncat, kriging_capi.F90:113-: 1 <= ncat <= nvar; variables past
+// ncat are secondary co-variates, left out of the normalisation
+int krige_ind_set_ncat(int64_t h, int ncat) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (!e->indicator) throw std::string("handle was not created by krige_ind_create");
+  if (ncat < 1 || ncat > e->nvar) throw std::string("ncat must satisfy 1 <= ncat <= nvar");
+  e->ncat = ncat;
+  KK_GUARD_END
+}
+
 // krige_destroy, kriging_capi_common.F90 (release_obj_base)
 int krige_destroy(int64_t* handle) {
   KK_GUARD_BEGIN
@@ -183,6 +206,7 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
   e->std_ck = std_ck;
   e->verbose = verbose;
   engine_free_weight_store(*e);
+  e->ncat = 0;
   e->store_weight = store_weight ? 1 : 0;
   e->use_old_weight = use_old_weight ? 1 : 0;
   e->bounds[0] = bounds ? bounds[0] : -DBL_MAX;

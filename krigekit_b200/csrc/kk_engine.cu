@@ -389,8 +389,23 @@ static void fill_params(Engine& e, SolveParams& P) {
   // the refinement form's correction term c is about (cond * eps32)^2 of its
   // value and carries an error of about c^1.5: c <= tol^(2/3) keeps it <= tol
   P.refine_tol_corr = std::cbrt(P.refine_tol * P.refine_tol);
-  if (P.pa + nv + 1 + ((P.ck_isa || P.sk_any) ? nv : 0) > 8)
-    throw std::string("too many drift/variable columns for the register kernels (max 8)");
+}
+
+// Systems with more drift / variable columns than the register kernels hold
+// (8: e.g. four-variable cokriging without standardisation) are solved by the
+// general kernel.
+static bool wide_columns(const SolveParams& P) {
+  return P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0) > 8;
+}
+
+// indicator kriging: the category probabilities after a solve or a re-estimate
+static void indicator_post(Engine& e) {
+  if (!e.indicator || e.nsim > 0) return;
+  const int kcat = (e.ncat > 0 && e.ncat <= e.nvar) ? e.ncat : e.nvar;
+  launch_indicator_post(e.est.as<double>(), e.nblock, e.nvar, kcat, sm_count(e.device), e.stream);
+  KK_CUDA(cudaGetLastError());
+  KK_CUDA(cudaStreamSynchronize(e.stream));
+  e.launches += 1;
 }
 
 static void engine_replay(Engine& e);
@@ -715,9 +730,12 @@ void engine_solve(Engine& e) {
       e.launches += 2;
     }
   };
+  const bool wide = wide_columns(P);
   timer.start();
-  run_list(e.bucket.as<int>() + (size_t)KK_CNT_B16 * nb, cb[KK_CNT_B16], 32, refine, KK_CNT_WORK0 + 0);
-  run_list(e.bucket.as<int>() + (size_t)KK_CNT_B64 * nb, cb[KK_CNT_B64], 64, refine, KK_CNT_WORK0 + 1);
+  if (!wide) {
+    run_list(e.bucket.as<int>() + (size_t)KK_CNT_B16 * nb, cb[KK_CNT_B16], 32, refine, KK_CNT_WORK0 + 0);
+    run_list(e.bucket.as<int>() + (size_t)KK_CNT_B64 * nb, cb[KK_CNT_B64], 64, refine, KK_CNT_WORK0 + 1);
+  }
   timer.stop(2);
   if (refine) {
     // targets whose FP32 factorisation failed or whose correction check did
@@ -737,11 +755,12 @@ void engine_solve(Engine& e) {
   KK_CUDA(cudaStreamSynchronize(st));
   // generic path: n > 64 bucket and Cholesky failures
   const int nbig = cnt[KK_CNT_BIG], nfb = cnt[KK_CNT_FB];
-  if (nbig > 0 || nfb > 0) {
+  const int nwide = wide ? std::max(cnt[KK_CNT_B16], cnt[KK_CNT_B64]) : 0;
+  if (nbig > 0 || nfb > 0 || nwide > 0) {
     int mtot = mm_total + P.pa;
     size_t stride = (size_t)mtot * mtot * 2 + (size_t)nv * mtot * 3 + (size_t)mtot * (P.pa + 2) +
                     (size_t)(P.pa + 1) * (P.pa + 1) + (size_t)(P.pa + 1) * nv + (size_t)mtot + 64;
-    const int nthreads = std::max(1, std::min(std::max(nbig, nfb), 2048));
+    const int nthreads = std::max(1, std::min(std::max(std::max(nbig, nfb), nwide), 2048));
     e.scratch.reserve(sizeof(double) * stride * nthreads);
     P.scratch = e.scratch.as<double>();
     P.scratch_stride = (int)stride;
@@ -753,6 +772,14 @@ void engine_solve(Engine& e) {
     if (nfb > 0) {
       launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(nfb, 2048), st);
       e.launches += 1;
+    }
+    if (wide) {
+      const int lists[2] = {KK_CNT_B16, KK_CNT_B64};
+      for (int sl : lists) {
+        if (cnt[sl] <= 0) continue;
+        launch_solve_generic(P, e.bucket.as<int>() + (size_t)sl * nb, sl, std::min(cnt[sl], 2048), st);
+        e.launches += 1;
+      }
     }
     KK_CUDA(cudaGetLastError());
     timer.stop(3);
@@ -773,6 +800,7 @@ void engine_solve(Engine& e) {
     e.wstore_dev = true;
     e.wstore_host = false;
   }
+  indicator_post(e);
   e.solved = true;
   e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -939,6 +967,7 @@ static void engine_replay(Engine& e) {
   KK_CUDA(cudaGetLastError());
   KK_CUDA(cudaStreamSynchronize(st));
   e.launches = 1;
+  indicator_post(e);
   std::memset(e.counters_last, 0, sizeof e.counters_last);
   e.solved = true;
 }

@@ -118,6 +118,8 @@ struct Engine {
   // solve, wbuf[(t * nvar + jv) * wstride + row] with rows in matrix order,
   // together with the neighbour lists of that solve; set_weights stages a
   // caller's store on the host until the next solve uploads it
+  int indicator = 0;  // krige_ind_create: probabilities normalised after each solve
+  int ncat = 0;       // indicator categories (0: every variable)
   int store_weight = 0, use_old_weight = 0;
   bool wstore_dev = false;   // the device holds a complete store
   bool wstore_host = false;  // set_weights data waiting for upload

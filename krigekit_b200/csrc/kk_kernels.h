@@ -106,6 +106,9 @@ void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
 // Estimates of every target from the weight store (P.wout, P.nbr, P.nnear)
 // and the current observation values (weight-store reuse).
 void launch_replay(const SolveParams& P, int nsm, cudaStream_t st);
+// Indicator kriging: clip the first kcat estimates per target to [0, 1] and
+// normalise them to sum to one.
+void launch_indicator_post(double* est, int nb, int nvar, int kcat, int nsm, cudaStream_t st);
 // Warp-per-target solve of the targets list[item0 + i], i < nitems (or
 // < *cnt - item0 when cnt is given): k_assemble writes each target's packed
 // K64 to Kg + i * N (N + 1) / 2, then k_solve_warp factors and solves; N is

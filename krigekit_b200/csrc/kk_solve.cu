@@ -147,6 +147,29 @@ __global__ void __launch_bounds__(256) k_replay(const __grid_constant__ SolvePar
   }
 }
 
+// post_solve_indicator (kriging_indicator.F90:170-185): the first kcat
+// estimates of every target (the category probabilities of indicator
+// kriging) clipped to [0, 1] and scaled to sum to one when the sum is
+// positive; NaN targets stay NaN.
+__global__ void k_indicator_post(double* __restrict__ est, int nb, int nvar, int kcat) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    double* v = est + (size_t)t * nvar;
+    double sum = 0.0;
+    for (int k = 0; k < kcat; ++k) {
+      const double c = fmax(0.0, fmin(1.0, v[k]));
+      v[k] = c;
+      sum += c;
+    }
+    if (sum > 0.0)
+      for (int k = 0; k < kcat; ++k) v[k] = v[k] / sum;
+  }
+}
+
+void launch_indicator_post(double* est, int nb, int nvar, int kcat, int nsm, cudaStream_t st) {
+  const int blocks = std::max(1, std::min((nb + 255) / 256, nsm * 8));
+  k_indicator_post<<<blocks, 256, 0, st>>>(est, nb, nvar, kcat);
+}
+
 void launch_replay(const SolveParams& P, int nsm, cudaStream_t st) {
   const int need = (P.nblock + 7) / 8;  // eight warps per block
   const int blocks = std::max(1, std::min(need, nsm * 8));

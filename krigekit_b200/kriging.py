@@ -58,6 +58,8 @@ def _iptr(a):
 class Kriging:
     """Spatial kriging / cokriging on one B200 (drop-in for krigekit.Kriging)."""
 
+    _CREATE = "krige_create"  # C-ABI constructor of the handle
+
     def __init__(
         self,
         ndim: int = 2,
@@ -94,7 +96,7 @@ class Kriging:
         dev = torch.cuda.current_device() if device is None else int(device)
         _lib.use_torch_allocator()
         h = ctypes.c_int64(0)
-        _lib.check(lib.krige_create(ctypes.byref(h)), "krige_create")
+        _lib.check(getattr(lib, self._CREATE)(ctypes.byref(h)), self._CREATE)
         self._handle = h.value
         self._lib = lib
         _lib.register(self)

@@ -331,3 +331,35 @@ def spacetime_kriging(obs_coord, obs_value, grid_coord, grid_time, spatial_spec,
     k.set_search(ivar=1, time_at=at, anis1=search_anis1, anis2=search_anis2, azimuth=search_azimuth)
     k.solve(nthread=nthread, ncache=ncache)
     return k.get_results()
+
+
+def spacetime_cokriging(obs_coords, obs_values, grid_coord, grid_time, spatial_specs: dict, temporal_specs: dict,
+                        joint_sills: dict, model: str = "sum_metric", transform: str = "linear", at: float = 1.0,
+                        time_nugget: float = 0.0, time_sill: float = 1.0, nmax: int = 20,
+                        maxdist: Optional[float] = None, nthread: int = 0, ncache: Optional[int] = None, **kw):
+    """One-shot ordinary space-time cokriging (kriging_st.py:1069-1130).
+
+    ``obs_coords`` / ``obs_values``: one array per variable, coordinates
+    ``(nobs_i, ndim + 1)`` with time last; ``spatial_specs`` /
+    ``temporal_specs``: (ivar, jvar) -> structure dict or list of dicts;
+    ``joint_sills``: (ivar, jvar) -> sills of the sum-metric model.
+    """
+    nvar = len(obs_coords)
+    k = SpaceTimeKriging(nvar=nvar, **kw)
+    k.set_st_model(model=model, transform=transform, at=at, time_nugget=time_nugget, time_sill=time_sill)
+    for i, (coord, value) in enumerate(zip(obs_coords, obs_values), start=1):
+        k.set_obs(ivar=i, coord=coord, value=value, nmax=nmax, maxdist=maxdist)
+    for (iv, jv), spec in spatial_specs.items():
+        for s in ([spec] if isinstance(spec, dict) else list(spec)):
+            k.set_vgm(iv, jv, **s)
+    for (iv, jv), spec in temporal_specs.items():
+        for s in ([spec] if isinstance(spec, dict) else list(spec)):
+            k.set_vgm_temporal(iv, jv, **s)
+    if model == "sum_metric":
+        for (iv, jv), sills in joint_sills.items():
+            k.set_vgm_joint_sills(iv, jv, *sills)
+    k.set_grid(coord=grid_coord, time=grid_time)
+    for i in range(1, nvar + 1):
+        k.set_search(ivar=i, time_at=at)
+    k.solve(nthread=nthread, ncache=ncache)
+    return k.get_results()
