@@ -197,11 +197,25 @@ int krige_get_status(int64_t handle, int nblocks, int *status);
 int krige_gpu_stats(int64_t handle, int *out8, double *solve_ms);
 
 /* No counterpart in the reference.  Raw device counters of the last solve, out[0..n), n <= 32:
- * [0..2] targets per size bucket (<= 32, 33..64, > 64 neighbours), [3] general-kernel
+ * [0..2] targets per size bucket (<= 32, 33..64, > 128 neighbours), [3] general-kernel
  * list, [4] FP32 systems re-solved in FP64, [5] failures (NaN), [6] Cholesky solves,
  * [7] LDL^T solves, [16..19] search fallbacks per variable, [20] refinement passes,
- * [21] LDL^T solves that needed the 1e-6 mean-diagonal jitter. */
+ * [21] LDL^T solves that needed the 1e-6 mean-diagonal jitter, [22] targets with
+ * 65..128 neighbours. */
 int krige_gpu_counters(int64_t handle, int n, int *out);
+/* No counterpart in the reference (its solver has one CPU path).  How krige_solve picks
+ * the kernel for each neighbour-count list (2..32, 33..64, > 128, 65..128 equations):
+ * mode 0 = fixed plan (warp per target up to 64, CTA per target up to 128, general kernel
+ * beyond), 1 = time the candidate kernels on a sample of each list once per system
+ * signature and keep the fastest (process-wide cache; the default), 2 = time them again
+ * on the next solve. */
+int krige_set_autotune(int64_t handle, int mode);
+/* Plan of the last solve: kernel4[list] = 0 warp/32, 1 warp/64, 2 CTA/128, 3 general,
+ * -1 empty list; us16[list * 4 + kernel] = tuner's microseconds per target (NaN where
+ * not timed).  Either pointer may be NULL. */
+int krige_get_kernel_plan(int64_t handle, int *kernel4, double *us16);
+/* Forget every cached plan (all handles). */
+int krige_autotune_clear(void);
 /* Enable per-phase CUDA-event timing of krige_solve (one event sync per phase). */
 int krige_gpu_profile(int64_t handle, int enable);
 /* Device ms per phase of the last solve: search, bucket, solve kernels, fallbacks;

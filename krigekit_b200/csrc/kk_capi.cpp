@@ -861,6 +861,37 @@ int krige_gpu_counters(int64_t h, int n, int* out) {
   KK_GUARD_END
 }
 
+// Kernel plan of the solve: 0 fixed, 1 tuned once per system signature, 2
+// tuned again on the next solve.
+int krige_set_autotune(int64_t h, int mode) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (mode < 0 || mode > 2) throw std::string("autotune mode must be 0, 1 or 2");
+  e->autotune = mode;
+  KK_GUARD_END
+}
+
+// Kernel per neighbour-count list in the last solve and the tuner's
+// microseconds per target of each candidate (NaN where not timed).
+int krige_get_kernel_plan(int64_t h, int* kernel4, double* us16) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  for (int li = 0; li < KK_NLIST; ++li) {
+    if (kernel4) kernel4[li] = e->plan[li];
+    for (int k = 0; k < KK_NKER; ++k)
+      if (us16) us16[li * KK_NKER + k] = e->plan_us[li][k];
+  }
+  KK_GUARD_END
+}
+
+int krige_autotune_clear(void) {
+  KK_GUARD_BEGIN
+  tune_clear();
+  KK_GUARD_END
+}
+
 // Enable per-phase CUDA-event timing of solve() (adds one event sync per phase).
 int krige_gpu_profile(int64_t h, int enable) {
   KK_GUARD_BEGIN

@@ -108,5 +108,14 @@ enum {
   KK_ST_LDLT = 8,        // Cholesky failed -> LDL^T path
   KK_ST_FAIL = 16,       // singular after jitter -> NaN
   KK_ST_EMPTY = 32,      // no neighbours
-  KK_ST_BIG = 64,        // more neighbours than the register kernels hold
+  KK_ST_BIG = 64,        // more neighbours than the register kernels hold (> 128)
 };
+
+// Neighbour-count lists written by the bucketing kernel, list li at
+// lists + li * nblock: 2..32, 33..64, > 128 and 65..128 equations
+enum { KK_LIST_B32 = 0, KK_LIST_B64 = 1, KK_LIST_BIG = 2, KK_LIST_B128 = 3, KK_NLIST = 4 };
+
+// Solve kernels a list can be planned on: warp per target holding 32 or 64
+// equations, CTA per target holding 128, and the general thread-per-target
+// kernel (any size)
+enum { KK_KER_W32 = 0, KK_KER_W64 = 1, KK_KER_BLOCK = 2, KK_KER_GEN = 3, KK_NKER = 4 };

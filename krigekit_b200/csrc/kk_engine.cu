@@ -6,9 +6,12 @@
 //   search     k_search per variable (+ exact kd-tree replica for targets
 //              whose selection boundary has equal distances)
 //   bucket     size buckets of npp per target
-//   solve      register kernels per bucket (FP64, or FP32 + FP64
-//              refinement), FP64 re-solve of non-converged targets, generic
-//              kernel for n > 64 and Cholesky failures (LDL^T + jitter)
+//   solve      per bucket the planned kernel: warp per target (FP64, or
+//              FP32 + FP64 refinement) up to 64 equations, CTA per target
+//              up to 128, generic kernel beyond (and for Cholesky failures:
+//              LDL^T + jitter); the plan can be tuned by timing candidates
+//              on a sample of each bucket; FP64 re-solve of non-converged
+//              FP32 targets
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,6 +19,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -408,6 +413,84 @@ static void indicator_post(Engine& e) {
   e.launches += 1;
 }
 
+// ---------------------------------------------------------------------------
+// solve plan: which kernel solves each neighbour-count list
+// ---------------------------------------------------------------------------
+// Equations a planned kernel holds (the assembly buffer's row count).
+static int kernel_rows(int ker) { return ker == KK_KER_W32 ? 32 : (ker == KK_KER_W64 ? 64 : 128); }
+// Targets per assembly chunk: about 1.1 GB of packed FP64 K per chunk.
+static int chunk_targets(int N) { return N == 128 ? (1 << 14) : (1 << 16); }
+static size_t kbuf_bytes(int N, int n) { return sizeof(double) * (size_t)n * (N * (N + 1) / 2); }
+
+// The plan without tuning: the smallest register kernel that holds the list,
+// the general kernel for systems wider than eight columns, for more than 128
+// equations, and for the weight store's 65..128 list (the CTA kernel keeps
+// no weights).
+static int default_kernel(int li, bool wide, bool wstore) {
+  if (wide || li == KK_LIST_BIG) return KK_KER_GEN;
+  if (li == KK_LIST_B32) return KK_KER_W32;
+  if (li == KK_LIST_B64) return KK_KER_W64;
+  return wstore ? KK_KER_GEN : KK_KER_BLOCK;
+}
+
+// Kernels that can solve list li: the default and the next larger one (a
+// list of at most 32 equations on the 64-row warp kernel, 33..64 on the CTA
+// kernel, 65..128 on the general kernel), so the tuner moves the bucket
+// boundaries by one step where that is faster.
+static int candidates(int li, bool wide, bool wstore, int* cand) {
+  const int d = default_kernel(li, wide, wstore);
+  cand[0] = d;
+  if (d == KK_KER_GEN) return 1;
+  if (d == KK_KER_W32) { cand[1] = KK_KER_W64; return 2; }
+  if (d == KK_KER_W64) {
+    if (wstore) return 1;
+    cand[1] = KK_KER_BLOCK;
+    return 2;
+  }
+  cand[1] = KK_KER_GEN;
+  return 2;
+}
+
+constexpr int KK_TUNE_MIN = 2048;     // shorter lists keep the fixed plan (unless cached)
+constexpr int KK_TUNE_SAMPLE = 8192;  // targets timed per candidate
+
+// System signature the tuner's choice is cached under: what changes the
+// work per target (form, columns, covariance path, dimensions, block
+// targets) and the list's size class (a short list does not fill the GPU).
+struct TuneKey {
+  int v[9];
+  bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 9, o.v, o.v + 9); }
+};
+struct TuneEntry {
+  int kernel = KK_KER_GEN;
+  double us[KK_NKER];
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneEntry> g_tune;
+
+static TuneKey tune_key(const SolveParams& P, int li, int refine, int st, int count) {
+  const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return TuneKey{{li, refine, C, P.nvar, P.fast_model, P.nlag + 8 * st, P.gstart ? 1 : 0,
+                  count >= 65536 ? 2 : (count >= 8192 ? 1 : 0), dev}};
+}
+static bool tune_find(const TuneKey& k, TuneEntry& out) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tune.find(k);
+  if (it == g_tune.end()) return false;
+  out = it->second;
+  return true;
+}
+static void tune_store(const TuneKey& k, const TuneEntry& e) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune[k] = e;
+}
+void tune_clear() {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune.clear();
+}
+
 static void engine_replay(Engine& e);
 
 void engine_solve(Engine& e) {
@@ -549,7 +632,7 @@ void engine_solve(Engine& e) {
   e.var.reserve(sizeof(double) * (size_t)nb * nv * nv);
   e.status.reserve(sizeof(int) * nb);
   e.counters.reserve(sizeof(int) * KK_CNT_N);
-  e.bucket.reserve(sizeof(int) * (size_t)nb * 3);
+  e.bucket.reserve(sizeof(int) * (size_t)nb * KK_NLIST);
   e.npp.reserve(sizeof(int) * (size_t)nb * 2);  // fb + fp64 lists
   KK_CUDA(cudaMemsetAsync(e.counters.p, 0, sizeof(int) * KK_CNT_N, st));
   KK_CUDA(cudaMemsetAsync(e.status.p, 0, sizeof(int) * nb, st));
@@ -716,13 +799,19 @@ void engine_solve(Engine& e) {
     P.wstride = mm_total;
   }
   const int refine = e.store_weight ? 0 : solve_refine_form(P, e.precision);
-  constexpr int CH = 1 << 16;
-  const int nk64 = 64 * 65 / 2;
-  const int most = std::max(cb[KK_CNT_B16], cb[KK_CNT_B64]);
-  if (most > 0) e.kbuf.reserve(sizeof(double) * (size_t)std::min(CH, most) * nk64);
+  const int mtot = mm_total + P.pa;
+  const size_t gstride = generic_stride(mtot, nv, P.pa);
+  auto generic_scratch = [&](int nthreads) {
+    e.scratch.reserve(sizeof(double) * gstride * std::max(1, std::min(nthreads, 2048)));
+    P.scratch = e.scratch.as<double>();
+    P.scratch_stride = (int)gstride;
+  };
+  // one chunk of a list: assembly into kbuf, then the factorisation kernel
   auto run_list = [&](const int* list, int count, int N, int form, int slot) {
-    for (int c0 = 0; c0 < count; c0 += CH) {
-      const int nit = std::min(CH, count - c0);
+    const int ch = chunk_targets(N);
+    if (count > 0) e.kbuf.reserve(std::max(e.kbuf.bytes, kbuf_bytes(N, std::min(ch, count))));
+    for (int c0 = 0; c0 < count; c0 += ch) {
+      const int nit = std::min(ch, count - c0);
       KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + slot, 0, sizeof(int), st));
       launch_assemble(P, N, list, nullptr, c0, nit, e.kbuf.as<double>(), nsm, st);
       launch_factor(P, form, N, list, nullptr, c0, nit, e.kbuf.as<double>(), slot, nsm, st);
@@ -730,56 +819,122 @@ void engine_solve(Engine& e) {
       e.launches += 2;
     }
   };
+  // the first count entries of a list on one kernel (the tuner's runs)
+  auto run_kernel = [&](int ker, const int* list, int count, int slot) {
+    if (ker == KK_KER_GEN) {
+      generic_scratch(count);
+      KK_CUDA(cudaMemcpyAsync(e.counters.as<int>() + KK_CNT_TUNE, &count, sizeof(int), cudaMemcpyHostToDevice, st));
+      launch_solve_generic(P, list, KK_CNT_TUNE, std::min(count, 2048), st);
+      KK_CUDA(cudaGetLastError());
+      e.launches += 1;
+    } else {
+      run_list(list, count, kernel_rows(ker), refine, slot);
+    }
+  };
+  // ---- kernel per neighbour-count list: fixed, or chosen by timing the
+  // candidates on a sample of the list (cached per system signature)
   const bool wide = wide_columns(P);
+  int* lists = e.bucket.as<int>();
+  for (int li = 0; li < KK_NLIST; ++li) {
+    const int count = cb[list_slot(li)];
+    e.plan[li] = count > 0 ? default_kernel(li, wide, e.store_weight != 0) : -1;
+    for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = NAN;
+    int cand[KK_NKER];
+    const int nc = candidates(li, wide, e.store_weight != 0, cand);
+    if (count <= 0 || nc < 2 || !e.autotune) continue;
+    const TuneKey key = tune_key(P, li, refine, e.st, count);
+    TuneEntry hit;
+    if (e.autotune == 1 && tune_find(key, hit)) {
+      e.plan[li] = hit.kernel;
+      for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = hit.us[k];
+      continue;
+    }
+    if (count < KK_TUNE_MIN) continue;
+    // the candidates' side effects (status bits, fallback lists, counters)
+    // are rolled back; the chosen kernel then solves the whole list
+    const int ns = std::min(count, KK_TUNE_SAMPLE);
+    int saved[KK_CNT_N];
+    KK_CUDA(cudaMemcpyAsync(saved, e.counters.p, sizeof saved, cudaMemcpyDeviceToHost, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    // the fallback lists hold nb entries: each run below appends at most ns
+    // to empty lists, and the counters are put back after every run
+    if (saved[KK_CNT_FB] != 0 || saved[KK_CNT_FP64] != 0) continue;
+    auto restore_counters = [&]() {
+      KK_CUDA(cudaMemcpyAsync(e.counters.p, saved, sizeof saved, cudaMemcpyHostToDevice, st));
+    };
+    e.tunebuf.reserve(sizeof(int) * (size_t)nb);
+    KK_CUDA(cudaMemcpyAsync(e.tunebuf.p, P.status, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToDevice, st));
+    const int* l = lists + (size_t)li * nb;
+    for (int c = 0; c < nc; ++c) {  // first launches (module loading) outside the timing
+      run_kernel(cand[c], l, std::min(ns, 256), KK_CNT_WORK0 + 3);
+      restore_counters();
+    }
+    cudaEvent_t ev[2];
+    KK_CUDA(cudaEventCreate(&ev[0]));
+    KK_CUDA(cudaEventCreate(&ev[1]));
+    TuneEntry ent;
+    ent.kernel = cand[0];
+    for (int k = 0; k < KK_NKER; ++k) ent.us[k] = NAN;
+    float best = 0.f;
+    for (int c = 0; c < nc; ++c) {
+      KK_CUDA(cudaEventRecord(ev[0], st));
+      run_kernel(cand[c], l, ns, KK_CNT_WORK0 + 3);
+      KK_CUDA(cudaEventRecord(ev[1], st));
+      KK_CUDA(cudaEventSynchronize(ev[1]));
+      float ms = 0.f;
+      KK_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      restore_counters();
+      ent.us[cand[c]] = 1e3 * ms / ns;
+      if (c == 0 || ms < best) { best = ms; ent.kernel = cand[c]; }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    KK_CUDA(cudaMemcpyAsync(P.status, e.tunebuf.p, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToDevice, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    e.tunebuf.release();
+    tune_store(key, ent);
+    e.plan[li] = ent.kernel;
+    for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = ent.us[k];
+  }
+  if (e.autotune == 2) e.autotune = 1;
   timer.start();
-  if (!wide) {
-    run_list(e.bucket.as<int>() + (size_t)KK_CNT_B16 * nb, cb[KK_CNT_B16], 32, refine, KK_CNT_WORK0 + 0);
-    run_list(e.bucket.as<int>() + (size_t)KK_CNT_B64 * nb, cb[KK_CNT_B64], 64, refine, KK_CNT_WORK0 + 1);
+  for (int li = 0; li < KK_NLIST; ++li) {
+    if (e.plan[li] < 0 || e.plan[li] == KK_KER_GEN) continue;
+    run_list(lists + (size_t)li * nb, cb[list_slot(li)], kernel_rows(e.plan[li]), refine, KK_CNT_WORK0 + li);
   }
   timer.stop(2);
   if (refine) {
     // targets whose FP32 factorisation failed or whose correction check did
-    // not pass: FP64 form
+    // not pass: FP64 form (they come from the lists of at most 64 equations)
     int nf = 0;
     KK_CUDA(cudaMemcpyAsync(&nf, e.counters.as<int>() + KK_CNT_FP64, sizeof(int), cudaMemcpyDeviceToHost, st));
     KK_CUDA(cudaStreamSynchronize(st));
     if (nf > 0) {
-      e.kbuf.reserve(std::max(e.kbuf.bytes, sizeof(double) * (size_t)std::min(CH, nf) * nk64));
       timer.start();
-      run_list(P.fp64_list, nf, 64, 0, KK_CNT_WORK0 + 2);
+      run_list(P.fp64_list, nf, 64, 0, KK_CNT_WORK0 + 4);
       timer.stop(3);
     }
   }
   int cnt[KK_CNT_N];
   KK_CUDA(cudaMemcpyAsync(cnt, e.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
   KK_CUDA(cudaStreamSynchronize(st));
-  // generic path: n > 64 bucket and Cholesky failures
-  const int nbig = cnt[KK_CNT_BIG], nfb = cnt[KK_CNT_FB];
-  const int nwide = wide ? std::max(cnt[KK_CNT_B16], cnt[KK_CNT_B64]) : 0;
-  if (nbig > 0 || nfb > 0 || nwide > 0) {
-    int mtot = mm_total + P.pa;
-    size_t stride = (size_t)mtot * mtot * 2 + (size_t)nv * mtot * 3 + (size_t)mtot * (P.pa + 2) +
-                    (size_t)(P.pa + 1) * (P.pa + 1) + (size_t)(P.pa + 1) * nv + (size_t)mtot + 64;
-    const int nthreads = std::max(1, std::min(std::max(std::max(nbig, nfb), nwide), 2048));
-    e.scratch.reserve(sizeof(double) * stride * nthreads);
-    P.scratch = e.scratch.as<double>();
-    P.scratch_stride = (int)stride;
+  // general kernel: the lists planned on it (more than 128 equations, wide
+  // systems, weight store) and Cholesky failures (LDL^T + jitter)
+  int ngen = cnt[KK_CNT_FB];
+  for (int li = 0; li < KK_NLIST; ++li)
+    if (e.plan[li] == KK_KER_GEN) ngen = std::max(ngen, cnt[list_slot(li)]);
+  if (ngen > 0) {
+    generic_scratch(ngen);
     timer.start();
-    if (nbig > 0) {
-      launch_solve_generic(P, e.bucket.as<int>() + (size_t)KK_CNT_BIG * nb, KK_CNT_BIG, std::min(nbig, 2048), st);
+    for (int li = 0; li < KK_NLIST; ++li) {
+      const int c = cnt[list_slot(li)];
+      if (e.plan[li] != KK_KER_GEN || c <= 0) continue;
+      launch_solve_generic(P, lists + (size_t)li * nb, list_slot(li), std::min(c, 2048), st);
       e.launches += 1;
     }
-    if (nfb > 0) {
-      launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(nfb, 2048), st);
+    if (cnt[KK_CNT_FB] > 0) {
+      launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(cnt[KK_CNT_FB], 2048), st);
       e.launches += 1;
-    }
-    if (wide) {
-      const int lists[2] = {KK_CNT_B16, KK_CNT_B64};
-      for (int sl : lists) {
-        if (cnt[sl] <= 0) continue;
-        launch_solve_generic(P, e.bucket.as<int>() + (size_t)sl * nb, sl, std::min(cnt[sl], 2048), st);
-        e.launches += 1;
-      }
     }
     KK_CUDA(cudaGetLastError());
     timer.stop(3);
@@ -1085,7 +1240,7 @@ void engine_release(Engine& e) {
   for (auto& b : e.tx) b.release();
   for (auto& b : e.gx) b.release();
   e.trs.release(); e.tln.release(); e.tdrift.release(); e.gstart.release(); e.gw.release();
-  e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release();
+  e.est.release(); e.var.release(); e.status.release(); e.npp.release(); e.bucket.release(); e.tunebuf.release();
   e.counters.release(); e.scratch.release(); e.kbuf.release(); e.til.release(); e.wbuf.release();
   if (e.hstage) cudaFreeHost(e.hstage);
   e.hstage = nullptr;

@@ -112,6 +112,15 @@ struct Engine {
   int profile = 0;
   double phase_ms[4] = {0, 0, 0, 0};
   int launches = 0;
+  // solve kernel per neighbour-count list (KK_KER_*, -1 for an empty list)
+  // in the last solve, and the tuner's measured microseconds per target of
+  // each candidate (NaN where not timed).  autotune: 0 fixed plan, 1 time
+  // the candidates once per system signature (process-wide cache), 2 time
+  // them again on the next solve
+  int autotune = 1;
+  int plan[KK_NLIST] = {-1, -1, -1, -1};
+  double plan_us[KK_NLIST][KK_NKER] = {};
+  DBuf tunebuf;  // status copy while the tuner runs
 
   // weight store (store_weight / use_old_weight, kriging_base.F90:2703-2990):
   // the weights of every target stay on the device after a store_weight
@@ -152,6 +161,8 @@ void engine_solve(Engine& e);
 // observation values of variable ivar first when it is not null.
 void engine_resolve_static(Engine& e, int ivar, int nobs, const double* value);
 void engine_release(Engine& e);
+// forget every cached kernel plan (krige_autotune_clear)
+void tune_clear();
 // weight store (kk_engine.cu): nm = largest neighbour-list length over the
 // variables; the getters copy the device store (or the staged one) into the
 // reference's column-major layouts

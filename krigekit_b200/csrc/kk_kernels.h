@@ -79,7 +79,7 @@ struct SolveParams {
 enum {
   KK_CNT_B16 = 0,   // bucket sizes (targets with npp in 2..32)
   KK_CNT_B64 = 1,   // npp in 33..64
-  KK_CNT_BIG = 2,   // npp > 64
+  KK_CNT_BIG = 2,   // npp > 128
   KK_CNT_FB = 3,    // generic fallback list length
   KK_CNT_FP64 = 4,  // FP32 targets re-solved in FP64
   KK_CNT_FAIL = 5,
@@ -89,8 +89,13 @@ enum {
   KK_CNT_REDO = 16,  // search tie/overflow count per variable (16..19)
   KK_CNT_ITER = 20,  // total refinement iterations
   KK_CNT_JITTER = 21,  // LDL^T systems solved after the 1e-6 mean-diagonal jitter
+  KK_CNT_B128 = 22,    // npp in 65..128
+  KK_CNT_TUNE = 23,    // list length of a kernel-tuning sample
   KK_CNT_N = 32
 };
+
+// the counter that holds the length of neighbour-count list li (KK_LIST_*)
+__host__ __device__ inline int list_slot(int li) { return li == KK_LIST_B128 ? (int)KK_CNT_B128 : li; }
 
 void launch_search_coords(const KkSearch& S, const double* const* x, double* scu, int n, cudaStream_t st);
 void launch_grid_build(const KkGrid& g, const double* scu, int* cell_of, int* count, int* start, int* cursor,
@@ -109,11 +114,12 @@ void launch_replay(const SolveParams& P, int nsm, cudaStream_t st);
 // Indicator kriging: clip the first kcat estimates per target to [0, 1] and
 // normalise them to sum to one.
 void launch_indicator_post(double* est, int nb, int nvar, int kcat, int nsm, cudaStream_t st);
-// Warp-per-target solve of the targets list[item0 + i], i < nitems (or
+// Register-kernel solve of the targets list[item0 + i], i < nitems (or
 // < *cnt - item0 when cnt is given): k_assemble writes each target's packed
-// K64 to Kg + i * N (N + 1) / 2, then k_solve_warp factors and solves; N is
-// 32 or 64 (neighbour-count bucket); slot is the work counter, which must
-// start at zero.
+// K64 to Kg + i * N (N + 1) / 2, then the factorisation kernel factors and
+// solves; N is 32 or 64 (k_solve_warp, a warp per target) or 128
+// (k_solve_block, a CTA per target, FP64 only); slot is the work counter,
+// which must start at zero.
 void launch_assemble(const SolveParams& P, int N, const int* list, const int* cnt, int item0, int nitems,
                      double* Kg, int nsm, cudaStream_t st);
 void launch_factor(const SolveParams& P, int refine, int N, const int* list, const int* cnt, int item0, int nitems,

@@ -13,6 +13,9 @@
 //                     warp per target: covariance matrix, register Cholesky,
 //                     right-hand sides forward-substituted in the same sweep;
 //                     FP64, or FP32 factor with an FP64 residual correction
+//   k_solve_block (kk_block.cuh)
+//                     CTA per target for 65..128 equations: the same register
+//                     layout over four warps, FP64
 //   k_solve_generic   one thread per target in global workspace: Cholesky
 //                     failures (Bunch-Kaufman LDL^T + jitter retry) and the
 //                     allocation-free re-solve
@@ -63,22 +66,22 @@ __global__ void k_bucket(SolveParams P, int* __restrict__ lists) {
       P.status[t] |= KK_ST_EMPTY;
       if (npp == 0 && !P.neglect_error) atomicAdd(&P.counters[KK_CNT_FAIL], 1);
     } else {
-      slot = npp <= 32 ? KK_CNT_B16 : (npp <= 64 ? KK_CNT_B64 : KK_CNT_BIG);
-      if (slot == KK_CNT_BIG) P.status[t] |= KK_ST_BIG;
+      slot = npp <= 32 ? KK_LIST_B32 : (npp <= 64 ? KK_LIST_B64 : (npp <= 128 ? KK_LIST_B128 : KK_LIST_BIG));
+      if (slot == KK_LIST_BIG) P.status[t] |= KK_ST_BIG;
     }
   }
   // one atomic per warp and list (the order within a list is free: every
   // target is solved on its own)
   const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int sl = KK_CNT_B16; sl <= KK_CNT_BIG; ++sl) {
-    const unsigned m = __ballot_sync(0xffffffffu, slot == sl);
+  for (int li = 0; li < KK_NLIST; ++li) {
+    const unsigned m = __ballot_sync(0xffffffffu, slot == li);
     if (!m) continue;
     const int leader = __ffs(m) - 1;
     int base = 0;
-    if (lane == leader) base = atomicAdd(&P.counters[sl], __popc(m));
+    if (lane == leader) base = atomicAdd(&P.counters[list_slot(li)], __popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
-    if (slot == sl) lists[(size_t)sl * P.nblock + base + __popc(m & lt)] = t;
+    if (slot == li) lists[(size_t)li * P.nblock + base + __popc(m & lt)] = t;
   }
 }
 
@@ -179,6 +182,7 @@ void launch_replay(const SolveParams& P, int nsm, cudaStream_t st) {
 }  // namespace kk
 
 #include "kk_warp.cuh"
+#include "kk_block.cuh"
 
 namespace kk {
 
@@ -575,6 +579,17 @@ static void launch_warp(const SolveParams& P, const int* list, const int* cnt, i
   k_solve_warp<T, N, REFINE, CB, WT><<<blocks, 32 * WPC, smem, st>>>(P, list, cnt, item0, nitems, Kg, slot);
 }
 
+template <int CB>
+static void launch_block(const SolveParams& P, const int* list, const int* cnt, int item0, int nitems,
+                         const double* Kg, int slot, int nsm, cudaStream_t st) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_block<CB>, 128, 0);
+  if (occ < 1) occ = 1;
+  int blocks = nsm * occ;
+  if (nitems < blocks) blocks = nitems > 0 ? nitems : 1;
+  k_solve_block<CB><<<blocks, 128, 0, st>>>(P, list, cnt, item0, nitems, Kg, slot);
+}
+
 int solve_refine_form(const SolveParams& P, int precision) {
   const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
   return precision != 0 && C <= KK_REFINE_COLS;
@@ -582,12 +597,20 @@ int solve_refine_form(const SolveParams& P, int precision) {
 
 void launch_assemble(const SolveParams& P, int N, const int* list, const int* cnt, int item0, int nitems,
                      double* Kg, int nsm, cudaStream_t st) {
-  int blocks = nsm * 3;  // the launch bound's residency
-  const int need = (nitems + 7) / 8;
+  // the launch bound's residency: three CTAs of eight warps (six of four
+  // for N = 128)
+  const int wpc = N == 128 ? 4 : 8;
+  int blocks = nsm * (N == 128 ? 6 : 3);
+  const int need = (nitems + wpc - 1) / wpc;
   if (need < blocks) blocks = need > 0 ? need : 1;
   // the fast covariance variant is a template parameter (the general path
   // runs in the first instantiation with P.fast_model == 0)
-  if (N == 32) {
+  if (N == 128) {
+    if (P.fast_model == 2) k_assemble<128, 2><<<blocks, 128, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else if (P.fast_model == 3) k_assemble<128, 3><<<blocks, 128, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else if (P.fast_model == 4) k_assemble<128, 4><<<blocks, 128, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+    else k_assemble<128, 1><<<blocks, 128, 0, st>>>(P, list, cnt, item0, nitems, Kg);
+  } else if (N == 32) {
     if (P.fast_model == 2) k_assemble<32, 2><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else if (P.fast_model == 3) k_assemble<32, 3><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
     else if (P.fast_model == 4) k_assemble<32, 4><<<blocks, 256, 0, st>>>(P, list, cnt, item0, nitems, Kg);
@@ -604,7 +627,12 @@ void launch_factor(const SolveParams& P, int refine, int N, const int* list, con
                    const double* Kg, int slot, int nsm, cudaStream_t st) {
   const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
   const bool narrow = C <= 3;
-  if (refine) {
+  if (N == 128) {
+    // CTA per target, FP64 (no weight-store form: those targets take the
+    // general kernel)
+    if (narrow) launch_block<3>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+    else launch_block<MAXC>(P, list, cnt, item0, nitems, Kg, slot, nsm, st);
+  } else if (refine) {
     // the refinement's sweeps and residual cost in proportion to the columns
     // carried: 3 (one variable, ordinary or simple), 5 (drift or two-variable
     // cokriging), 6

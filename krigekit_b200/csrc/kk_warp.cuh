@@ -113,6 +113,8 @@ __device__ __forceinline__ void sweep_fwd(T (&v)[RM][CB], const float* __restric
 // list[item0 + i], i < count, written packed row-major lower to
 // Kg + i * N (N + 1) / 2.  One warp per target; the packed entries are
 // spread evenly over the lanes (stores are contiguous across the warp).
+// Eight warps per CTA (four for N = 128, to stay within 48 KB of static
+// shared memory).
 // This is the part of the solve that is bound by covariance-table latency,
 // so it runs as its own kernel with many resident warps; the factorisation
 // kernel then reads K from this buffer.  On the fast covariance paths an
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
     int obs[N];
     int var[N];
   };
-  __shared__ Rows rows[8];
+  __shared__ Rows rows[N == 128 ? 4 : 8];
   __shared__ PairModel s_pm[4];  // two-variable fast path (FM 3), dynamic pair index
   if (FM == 3 && threadIdx.x < 4) {
     PairModel& m = s_pm[threadIdx.x];

@@ -55,6 +55,26 @@ def _iptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
+
+KERNELS = ("warp32", "warp64", "block128", "general")
+PLAN_LISTS = ("npp<=32", "npp<=64", "npp>128", "npp<=128")
+
+
+def kernel_plan(handle) -> dict:
+    """{list: {"kernel": name, "us_per_target": {candidate: us}}} of the last
+    solve of a handle (krige_get_kernel_plan); empty lists are left out."""
+    ker = (ctypes.c_int * 4)()
+    us = (ctypes.c_double * 16)()
+    _lib.call("krige_get_kernel_plan", handle, ker, us)
+    out = {}
+    for li, name in enumerate(PLAN_LISTS):
+        if ker[li] < 0:
+            continue
+        timed = {KERNELS[k]: us[li * 4 + k] for k in range(4) if us[li * 4 + k] == us[li * 4 + k]}
+        out[name] = {"kernel": KERNELS[ker[li]], "us_per_target": timed}
+    return out
+
+
 class Kriging:
     """Spatial kriging / cokriging on one B200 (drop-in for krigekit.Kriging)."""
 
@@ -291,9 +311,27 @@ class Kriging:
         """Raw device counters of the last solve (extension; krige_gpu_counters)."""
         buf = (ctypes.c_int * 32)()
         _lib.call("krige_gpu_counters", self._h(), 32, buf)
-        return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt64": buf[2], "general_list": buf[3],
+        return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt128": buf[2], "bucket_le128": buf[22],
+                "general_list": buf[3],
                 "fp64_resolve": buf[4], "fail": buf[5], "chol": buf[6], "ldlt": buf[7],
                 "search_redo": [buf[16 + v] for v in range(4)], "refine_passes": buf[20], "jitter": buf[21]}
+
+    def set_autotune(self, mode: int = 1):
+        """Kernel choice per neighbour-count list (extension; krige_set_autotune):
+        0 fixed, 1 timed once per system signature (default), 2 timed again on
+        the next solve."""
+        _lib.call("krige_set_autotune", self._h(), int(mode))
+
+    def kernel_plan(self) -> dict:
+        """Kernel that solved each non-empty neighbour-count list in the last
+        solve, with the tuner's microseconds per target of every timed
+        candidate (extension; krige_get_kernel_plan)."""
+        return kernel_plan(self._h())
+
+    @staticmethod
+    def autotune_clear():
+        """Forget every cached kernel plan (extension; krige_autotune_clear)."""
+        _lib.call("krige_autotune_clear")
 
     def profile(self, enable: bool = True):
         """Record per-phase device time of each solve (extension)."""

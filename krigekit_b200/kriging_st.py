@@ -263,9 +263,19 @@ class SpaceTimeKriging:
         """Raw device counters of the last solve (extension; krige_gpu_counters)."""
         buf = (ctypes.c_int * 32)()
         _lib.call("krige_gpu_counters", self._h(), 32, buf)
-        return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt64": buf[2], "general_list": buf[3],
+        return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt128": buf[2], "bucket_le128": buf[22],
+                "general_list": buf[3],
                 "fp64_resolve": buf[4], "fail": buf[5], "chol": buf[6], "ldlt": buf[7],
                 "search_redo": [buf[16 + v] for v in range(4)], "refine_passes": buf[20], "jitter": buf[21]}
+
+    def set_autotune(self, mode: int = 1):
+        """Kernel choice per neighbour-count list (extension; krige_set_autotune)."""
+        _lib.call("krige_set_autotune", self._h(), int(mode))
+
+    def kernel_plan(self) -> dict:
+        """Kernel per neighbour-count list of the last solve (extension)."""
+        from .kriging import kernel_plan
+        return kernel_plan(self._h())
 
     def profile(self, enable: bool = True):
         _lib.call("krige_gpu_profile", self._h(), int(bool(enable)))

@@ -1,7 +1,8 @@
 """GPU parity on edge cases of the solve path, against the CPU oracle.
 
 Sparse neighbourhoods (maxdist leaves targets with 0, 1 or a few neighbours,
-with and without nmin), neighbourhoods above 64 (the general kernel), simple
+with and without nmin), neighbourhoods above 64 (the CTA-per-target and the
+general kernel), simple
 kriging, Gauss-quadrature blocks, 3-D sector search, per-target range scale
 and local nugget, 1-D kriging, and the error raised for duplicate
 observations.  Same bar as the other parity tests: identical neighbour sets,
@@ -74,12 +75,14 @@ def test_sparse_neighbourhoods(precision, nmin):
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
-def test_large_neighbourhood_general_kernel(precision):
+@pytest.mark.parametrize("nmax", [100, 150])
+def test_large_neighbourhood(precision, nmax):
+    """100 neighbours: the CTA-per-target kernel; 150: the general kernel."""
     x, z = _field(12, 4000)
     grid = np.random.default_rng(5).uniform(0.1, 0.9, (300, 2))
 
     def setup(k):
-        k.set_obs(1, x, z, nmax=100)
+        k.set_obs(1, x, z, nmax=nmax)
         k.set_vgm(1, 1, "exp", nugget=0.02, sill=1.0, a_major=0.2)
         k.set_grid(grid)
         k.set_search(1)
@@ -87,7 +90,9 @@ def test_large_neighbourhood_general_kernel(precision):
 
     g, o = _pair(precision, setup, ndim=2, nvar=1)
     _check(g, o, float(np.std(z)), 1.02, TOL[precision])
-    assert (g.get_neighbours(1)[0] > 64).all()
+    assert (g.get_neighbours(1)[0] == nmax).all()
+    c = g.gpu_counters()
+    assert c["bucket_le128" if nmax <= 128 else "bucket_gt128"] == len(grid), c
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
