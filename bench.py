@@ -10,7 +10,11 @@ size (default 2, the benchmark); the JSON line has the same keys for each.
 Prints one JSON line.  ``value`` is device throughput of the FP32-factor +
 FP64-refinement form with inputs resident in HBM (CUDA events on the solve
 stream, L2 flushed between timed steps, max over ranks); ``fp64_plain`` is the
-same measurement for the FP64 form; ``e2e`` is the same metric through the
+same measurement for the FP64 form and ``auto_default`` for the library's
+default precision (per neighbour-count list the faster form, as timed by the
+kernel tuner); ``replay`` times the weight-store re-estimate (store_weight
+solve once, then update_obs_value + solve per step: one gather-dot kernel);
+``e2e`` is the same metric through the
 public ``Kriging`` API with host inputs/outputs copied every step.  The
 reference arm (``--impl reference``) times the CPU restatement of the
 reference engine (oracle/kk_oracle.c, OpenMP over all host threads) on a
@@ -215,10 +219,14 @@ def main():
                          "4 LMC cokriging, 5 space-time product-sum with block support")
     ap.add_argument("--grid", type=int, default=None,
                     help="targets per axis (default: the workload's own size, 2000 for the benchmark)")
+    ap.add_argument("--nmax", type=int, default=None,
+                    help="neighbours per variable (per sector), overriding the workload's own")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-auto", action="store_true", help="skip the leg of the default precision (auto)")
+    ap.add_argument("--no-replay", action="store_true", help="skip the weight-store re-estimate leg")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
                     help="form of the timed leg (fp64 is for profiling the plain form alone)")
     args = ap.parse_args()
@@ -229,7 +237,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        run_reference(args, bw.Workload(args.config, args.grid))
+        run_reference(args, bw.Workload(args.config, args.grid, args.nmax))
         return
 
     import torch
@@ -243,7 +251,7 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    W = bw.Workload(args.config, args.grid)
+    W = bw.Workload(args.config, args.grid, args.nmax)
     w = W.w
     nvar = w["nvar"]
     ntarget = W.ntarget
@@ -297,6 +305,7 @@ def main():
     ph32 = k32.phases()
     k32.profile(False)
     gst = k32.gpu_stats()
+    k32_plan = k32.kernel_plan()
     e32, v32 = k32.get_results()
     nb32 = neighbours(k32, nvar)
     nnear = sum(nn.astype(np.int64) for nn, _ in nb32)
@@ -321,18 +330,76 @@ def main():
             "var_max": float(ve[fin].max()), "var_p99": float(np.percentile(ve[fin], 99))}
         del k64
 
-    # ---- roofline of the dominant kernel (the FP32 solve kernels)
+    # ---- the product default: per list the form the kernel tuner timed faster
+    auto = None
+    if not args.no_auto and args.precision != "fp64":
+        ka = W.product("auto", idx=slab)
+        tota, _ = time_steps(ka, args.steps, args.warmup)
+        auto = {"value": ntarget * world * args.steps / tota, "ms_per_step": tota / args.steps * 1e3,
+                "plan": ka.kernel_plan()}
+        del ka
+
+    # ---- weight-store re-estimate: solve once with store_weight, then new
+    # observation values per step (update_obs_value + solve = one k_replay)
+    replay = None
+    if not args.no_replay and not W.st:
+        kr = W.product("fp64", idx=slab, store_weight=True)
+        kr.solve()
+        rng = np.random.default_rng(7)
+        vals = [np.asarray(o["value"]) * (1.0 + 0.01 * rng.standard_normal(len(o["value"]))) for o in w["obs"]]
+        for _ in range(args.warmup):
+            for iv, v in enumerate(vals, start=1):
+                kr.update_obs_value(iv, v)
+            kr.solve()
+        barrier()
+        rtimes = []
+        for _ in range(args.steps):
+            for iv, v in enumerate(vals, start=1):
+                kr.update_obs_value(iv, v)
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            kr.solve()
+            e1.record()
+            e1.synchronize()
+            rtimes.append(e0.elapsed_time(e1))
+        barrier()
+        rt = sum(rtimes) / 1e3
+        if dist is not None:
+            t = torch.tensor([rt], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            rt = float(t.item())
+        rnn = sum(kr.get_neighbours(iv)[0].astype(np.int64) for iv in range(1, nvar + 1))
+        # HBM bytes per re-estimate: per target and variable the weight rows
+        # (8 B per neighbour of every variable), the neighbour lists (4 B),
+        # nnear, and the estimate written; the observation values (a few MB)
+        # are served from L2 and not counted
+        rbytes = float(len(slab)) * (nvar * 8 * 1 + 4 * nvar) + float(rnn.sum()) * (8 * nvar + 4)
+        rgbs = rbytes / (rt / args.steps) / 1e9
+        hbm_gbs_r, hbm_src_r = hbm_peak()
+        replay = {"value": ntarget * world * args.steps / rt, "unit": "targets/s", "ms_per_step": rt / args.steps * 1e3,
+                  "launches_per_step": kr.phases()["launches"],
+                  "roofline": {"bound": "hbm", "achieved": rgbs, "peak": hbm_gbs_r, "unit": "GB/s",
+                               "frac": rgbs / hbm_gbs_r, "bytes_per_step": rbytes, "kernel": "k_replay",
+                               "peak_source": hbm_src_r}}
+        kr.close()
+        del kr
+
+    # ---- roofline of the dominant kernel (the factorisation kernels)
     peaks = measured_peaks(torch, dev)
     p_aug, q_rhs = W.pq()
     nn = nnear[nnear >= 2].astype(np.float64)
     flops = float(solve_flops(nn, p_aug, q_rhs).sum())
-    achieved = flops / (ph32["solve_ms"] / 1e3) / 1e12
+    # the factorisation launches alone (CUDA events around each launch in the
+    # profiled solve), not the whole solve phase with the assembly
+    factor_ms = ph32["factor_ms"] if ph32.get("factor_ms", 0.0) > 0 else ph32["solve_ms"]
+    achieved = flops / (factor_ms / 1e3) / 1e12
     hbm_gbs, hbm_src = hbm_peak()
     # search: algorithmic bytes = target coords + neighbour gathers (8*(coords+1) per neighbour) + list write
     ncoord = w["ndim"] + (1 if W.st else 0)
     search_bytes = len(slab) * 8 * ncoord + float(nn.sum()) * (8 * (ncoord + 1) + 4) + len(slab) * 4 * nvar
     search_gbs = search_bytes / (ph32["search_ms"] / 1e3) / 1e9
-    ncu_known = args.config == 2 and args.grid in (None, 2000)
+    ncu_known = args.config == 2 and args.grid in (None, 2000) and args.nmax is None
 
     # ---- CPU baseline (oracle on a bounded sample) + accuracy against it
     cpu = None
@@ -401,15 +468,21 @@ def main():
             "config": cfg,
             "fp64_plain": fp64,
             "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,
+            "auto_default": auto,
+            "replay": replay,
+            "kernel_plan": k32_plan,
             "accuracy": acc,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
                          "frac": achieved / peaks["fp32"],
                          "traffic": NCU_DRAM_BYTES_PER_TARGET["solve_fp32_refine"] * ntarget if ncu_known else None,
                          "traffic_note": ("ncu DRAM bytes per target (400x400 grid) x targets of the solve"
                                           if ncu_known else "no ncu capture of this workload"),
-                         "kernel": "k_solve_warp<float,32|64,refine> (solve phase, CUDA-core FP32)",
+                         "kernel": "factorisation launches of the plan (k_solve_warp / k_solve_block), "
+                                   "CUDA-core arithmetic",
                          "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live",
-                         "flops_per_solve": flops, "solve_ms": ph32["solve_ms"]},
+                         "flops_per_solve": flops, "factor_ms": factor_ms,
+                         "frac_of_fp64_peak": achieved / peaks["fp64"],
+                         "solve_ms": ph32["solve_ms"]},
             "roofline_search": {"bound": "hbm", "achieved": search_gbs, "peak": hbm_gbs, "unit": "GB/s",
                                 "frac": search_gbs / hbm_gbs,
                                 "traffic": NCU_DRAM_BYTES_PER_TARGET["search"] * ntarget if ncu_known else None,

@@ -231,7 +231,7 @@ class Workload:
     """One configuration at a given size, configured onto the product classes
     or the CPU oracle for any subset of its targets."""
 
-    def __init__(self, c, grid=None):
+    def __init__(self, c, grid=None, nmax=None):
         self.c = c
         if c == 1:
             self.w = config1(grid_n=grid or 100)
@@ -246,6 +246,10 @@ class Workload:
             self.w = config5(grid_n=grid or 512)
         else:
             raise ValueError(f"unknown configuration {c}")
+        if nmax is not None:  # neighbours per variable (per sector in sector search)
+            for o in self.w["obs"]:
+                o["nmax"] = int(nmax)
+            self.w["name"] += f"_nmax{int(nmax)}"
         self.st = bool(self.w.get("st", False))
         self.blocks = st_blocks(self.w) if self.st else None
         self.ntarget = len(self.w["grid"])
@@ -265,13 +269,14 @@ class Workload:
     def ndim(self):
         return self.w["ndim"]
 
-    def product(self, precision, nmin=None, idx=None):
+    def product(self, precision, nmin=None, idx=None, **extra):
         from krigekit_b200 import Kriging, SpaceTimeKriging
         nmin = self.w["nmin"] if nmin is None else nmin
         if self.st:
-            k = SpaceTimeKriging(nvar=1, precision=precision, nmin=nmin)
+            k = SpaceTimeKriging(nvar=1, precision=precision, nmin=nmin, **extra)
         else:
-            k = Kriging(ndim=self.w["ndim"], nvar=self.w["nvar"], precision=precision, nmin=nmin, **self.w["kw"])
+            k = Kriging(ndim=self.w["ndim"], nvar=self.w["nvar"], precision=precision, nmin=nmin, **self.w["kw"],
+                        **extra)
         return self.configure(k, idx)
 
     def oracle(self, nmin=None, idx=None):

@@ -176,7 +176,10 @@ int krige_st_set_search(int64_t handle, int ivar, double time_at, double anis1, 
                         double dip, double plunge, int sector_search);
 
 /* ---- extensions of the GPU library (no counterpart in the reference) ---- */
-/* 0 = FP64 throughout, 1 = FP32 factorisation with FP64 iterative refinement (default). */
+/* 0 = FP64 throughout, 1 = FP32 factorisation with an FP64 residual correction (systems of at
+ * most six right-hand-side columns; wider ones stay FP64), 2 = auto (default): per neighbour-count
+ * list the faster of the two as timed by the kernel tuner (FP64 when not tuned).  Every form
+ * meets 1e-6 relative accuracy; 0 meets the FP64 one. */
 int krige_set_precision(int64_t handle, int mode);
 /* Targets with fewer than nmin neighbours return NaN (0 = reference behaviour). */
 int krige_set_nmin(int64_t handle, int nmin);
@@ -211,9 +214,10 @@ int krige_gpu_counters(int64_t handle, int n, int *out);
  * on the next solve. */
 int krige_set_autotune(int64_t handle, int mode);
 /* Plan of the last solve: kernel4[list] = 0 warp/32, 1 warp/64, 2 CTA/128, 3 general,
- * -1 empty list; us16[list * 4 + kernel] = tuner's microseconds per target (NaN where
- * not timed).  Either pointer may be NULL. */
-int krige_get_kernel_plan(int64_t handle, int *kernel4, double *us16);
+ * 4 warp/32 FP32 + correction, 5 warp/64 FP32 + correction, -1 empty list;
+ * us24[list * 6 + kernel] = tuner's microseconds per target (NaN where not timed).
+ * Either pointer may be NULL. */
+int krige_get_kernel_plan(int64_t handle, int *kernel4, double *us24);
 /* Forget every cached plan (all handles). */
 int krige_autotune_clear(void);
 /* Enable per-phase CUDA-event timing of krige_solve (one event sync per phase). */
@@ -221,6 +225,9 @@ int krige_gpu_profile(int64_t handle, int enable);
 /* Device ms per phase of the last solve: search, bucket, solve kernels, fallbacks;
  * launches = kernels launched by that solve. */
 int krige_gpu_phases(int64_t handle, double *out4, int *launches);
+/* Device ms of the last profiled solve's assembly launches (out2[0]) and factorisation
+ * launches (out2[1]) of the register kernels, each timed on its own. */
+int krige_gpu_kernel_ms(int64_t handle, double *out2);
 
 /* No counterpart in the reference.  Allocation-free FP64 re-solve: repeats the
  * last krige_solve of this handle with the same neighbour sets, after replacing

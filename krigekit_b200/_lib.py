@@ -91,6 +91,7 @@ SIGNATURES = {
     "krige_get_kernel_plan": ([_c_i64, _p_int, _p_dbl], _c_int),
     "krige_autotune_clear": ([], _c_int),
     "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),
+    "krige_gpu_kernel_ms": ([_c_i64, _p_dbl], _c_int),
     "krige_resolve_static": ([_c_i64, _c_int, _c_int, _p_dbl], _c_int),
     # in-memory weight store (reference layouts, kriging.py:259-274)
     "krige_get_weight_dims": ([_c_i64, _p_int, _p_int, _p_int], _c_int),

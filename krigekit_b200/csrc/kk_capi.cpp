@@ -670,7 +670,7 @@ int krige_set_precision(int64_t h, int mode) {
   KK_GUARD_BEGIN
   Engine* e = get(h);
   if (!e) return 1;
-  if (mode != 0 && mode != 1) throw std::string("precision mode must be 0 (fp64) or 1 (fp32_refine)");
+  if (mode < 0 || mode > 2) throw std::string("precision mode must be 0 (fp64), 1 (fp32_refine) or 2 (auto)");
   e->precision = mode;
   KK_GUARD_END
 }
@@ -830,7 +830,8 @@ const char* krige_to_str(int64_t h) {
   line("LOO-Cross Validation  ", yn(e->cross_validation));
   line("Use Old Weights       ", yn(e->use_old_weight));
   line("Store Weights         ", yn(e->store_weight));
-  line("Precision             ", e->precision ? "FP32 factor + FP64 correction" : "FP64");
+  line("Precision             ", e->precision == 2 ? "auto (FP64 or FP32 factor + FP64 correction, tuned)"
+                                : (e->precision ? "FP32 factor + FP64 correction" : "FP64"));
   snprintf(buf, sizeof buf, "%.17g", e->bounds[0]);
   line("Lower Bound           ", buf);
   snprintf(buf, sizeof buf, "%.17g", e->bounds[1]);
@@ -874,14 +875,14 @@ int krige_set_autotune(int64_t h, int mode) {
 
 // Kernel per neighbour-count list in the last solve and the tuner's
 // microseconds per target of each candidate (NaN where not timed).
-int krige_get_kernel_plan(int64_t h, int* kernel4, double* us16) {
+int krige_get_kernel_plan(int64_t h, int* kernel4, double* us24) {
   KK_GUARD_BEGIN
   Engine* e = get(h);
   if (!e) return 1;
   for (int li = 0; li < KK_NLIST; ++li) {
     if (kernel4) kernel4[li] = e->plan[li];
     for (int k = 0; k < KK_NKER; ++k)
-      if (us16) us16[li * KK_NKER + k] = e->plan_us[li][k];
+      if (us24) us24[li * KK_NKER + k] = e->plan_us[li][k];
   }
   KK_GUARD_END
 }
@@ -909,6 +910,17 @@ int krige_gpu_phases(int64_t h, double* out4, int* launches) {
   if (!e) return 1;
   for (int i = 0; i < 4; ++i) out4[i] = e->phase_ms[i];
   if (launches) *launches = e->launches;
+  KK_GUARD_END
+}
+
+// Device ms of the assembly and the factorisation launches of the last
+// profiled solve (both inside the solve and fallback phases).
+int krige_gpu_kernel_ms(int64_t h, double* out2) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  out2[0] = e->phase_ms[4];
+  out2[1] = e->phase_ms[5];
   KK_GUARD_END
 }
 

@@ -116,6 +116,15 @@ enum {
 enum { KK_LIST_B32 = 0, KK_LIST_B64 = 1, KK_LIST_BIG = 2, KK_LIST_B128 = 3, KK_NLIST = 4 };
 
 // Solve kernels a list can be planned on: warp per target holding 32 or 64
-// equations, CTA per target holding 128, and the general thread-per-target
-// kernel (any size)
-enum { KK_KER_W32 = 0, KK_KER_W64 = 1, KK_KER_BLOCK = 2, KK_KER_GEN = 3, KK_NKER = 4 };
+// equations (FP64, or FP32 factor + FP64 correction: the R forms), CTA per
+// target holding 128 (FP64), and the general thread-per-target kernel (FP64,
+// any size)
+enum {
+  KK_KER_W32 = 0,
+  KK_KER_W64 = 1,
+  KK_KER_BLOCK = 2,
+  KK_KER_GEN = 3,
+  KK_KER_W32R = 4,
+  KK_KER_W64R = 5,
+  KK_NKER = 6
+};

@@ -416,39 +416,58 @@ static void indicator_post(Engine& e) {
 // ---------------------------------------------------------------------------
 // solve plan: which kernel solves each neighbour-count list
 // ---------------------------------------------------------------------------
-// Equations a planned kernel holds (the assembly buffer's row count).
-static int kernel_rows(int ker) { return ker == KK_KER_W32 ? 32 : (ker == KK_KER_W64 ? 64 : 128); }
+// Equations a planned kernel holds (the assembly buffer's row count), and
+// its form (1: FP32 factor + FP64 correction).
+static int kernel_rows(int ker) {
+  return (ker == KK_KER_W32 || ker == KK_KER_W32R) ? 32 : ((ker == KK_KER_W64 || ker == KK_KER_W64R) ? 64 : 128);
+}
+static int kernel_form(int ker) { return (ker == KK_KER_W32R || ker == KK_KER_W64R) ? 1 : 0; }
 // Targets per assembly chunk: about 1.1 GB of packed FP64 K per chunk.
 static int chunk_targets(int N) { return N == 128 ? (1 << 14) : (1 << 16); }
 static size_t kbuf_bytes(int N, int n) { return sizeof(double) * (size_t)n * (N * (N + 1) / 2); }
 
+// rform: the warp kernels' forms open to a solve: 0 FP64 only (precision
+// fp64, the weight store, or more than six columns), 1 FP32 + correction,
+// 2 either (precision auto: FP64 unless the tuner times the other faster).
+//
 // The plan without tuning: the smallest register kernel that holds the list,
 // the general kernel for systems wider than eight columns, for more than 128
 // equations, and for the weight store's 65..128 list (the CTA kernel keeps
 // no weights).
-static int default_kernel(int li, bool wide, bool wstore) {
+static int default_kernel(int li, bool wide, bool wstore, int rform) {
   if (wide || li == KK_LIST_BIG) return KK_KER_GEN;
-  if (li == KK_LIST_B32) return KK_KER_W32;
-  if (li == KK_LIST_B64) return KK_KER_W64;
+  if (li == KK_LIST_B32) return rform == 1 ? KK_KER_W32R : KK_KER_W32;
+  if (li == KK_LIST_B64) return rform == 1 ? KK_KER_W64R : KK_KER_W64;
   return wstore ? KK_KER_GEN : KK_KER_BLOCK;
 }
 
-// Kernels that can solve list li: the default and the next larger one (a
-// list of at most 32 equations on the 64-row warp kernel, 33..64 on the CTA
+// Kernels that can solve list li: the default, the next larger one (a list
+// of at most 32 equations on the 64-row warp kernel, 33..64 on the CTA
 // kernel, 65..128 on the general kernel), so the tuner moves the bucket
-// boundaries by one step where that is faster.
-static int candidates(int li, bool wide, bool wstore, int* cand) {
-  const int d = default_kernel(li, wide, wstore);
-  cand[0] = d;
-  if (d == KK_KER_GEN) return 1;
-  if (d == KK_KER_W32) { cand[1] = KK_KER_W64; return 2; }
-  if (d == KK_KER_W64) {
-    if (wstore) return 1;
-    cand[1] = KK_KER_BLOCK;
-    return 2;
+// boundaries by one step where that is faster, and under rform 2 both forms
+// of each warp kernel.
+static int candidates(int li, bool wide, bool wstore, int rform, int* cand) {
+  const int d = default_kernel(li, wide, wstore, rform);
+  int n = 0;
+  cand[n++] = d;
+  if (d == KK_KER_GEN) return n;
+  if (li == KK_LIST_B32) {
+    if (rform == 2) {
+      cand[n++] = KK_KER_W32R;
+      cand[n++] = KK_KER_W64;
+      cand[n++] = KK_KER_W64R;
+    } else {
+      cand[n++] = rform == 1 ? KK_KER_W64R : KK_KER_W64;
+    }
+    return n;
   }
-  cand[1] = KK_KER_GEN;
-  return 2;
+  if (li == KK_LIST_B64) {
+    if (rform == 2) cand[n++] = KK_KER_W64R;
+    if (!wstore) cand[n++] = KK_KER_BLOCK;
+    return n;
+  }
+  cand[n++] = KK_KER_GEN;
+  return n;
 }
 
 constexpr int KK_TUNE_MIN = 2048;     // shorter lists keep the fixed plan (unless cached)
@@ -468,11 +487,11 @@ struct TuneEntry {
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneEntry> g_tune;
 
-static TuneKey tune_key(const SolveParams& P, int li, int refine, int st, int count) {
+static TuneKey tune_key(const SolveParams& P, int li, int rform, int st, int count) {
   const int C = P.pa + P.nvar + 1 + ((P.ck_isa || P.sk_any) ? P.nvar : 0);
   int dev = 0;
   cudaGetDevice(&dev);
-  return TuneKey{{li, refine, C, P.nvar, P.fast_model, P.nlag + 8 * st, P.gstart ? 1 : 0,
+  return TuneKey{{li, rform, C, P.nvar, P.fast_model, P.nlag + 8 * st, P.gstart ? 1 : 0,
                   count >= 65536 ? 2 : (count >= 8192 ? 1 : 0), dev}};
 }
 static bool tune_find(const TuneKey& k, TuneEntry& out) {
@@ -798,7 +817,7 @@ void engine_solve(Engine& e) {
     P.wout = e.wbuf.as<double>();
     P.wstride = mm_total;
   }
-  const int refine = e.store_weight ? 0 : solve_refine_form(P, e.precision);
+  const int rform = (e.store_weight || !solve_refine_form(P, e.precision)) ? 0 : e.precision;
   const int mtot = mm_total + P.pa;
   const size_t gstride = generic_stride(mtot, nv, P.pa);
   auto generic_scratch = [&](int nthreads) {
@@ -807,14 +826,20 @@ void engine_solve(Engine& e) {
     P.scratch_stride = (int)gstride;
   };
   // one chunk of a list: assembly into kbuf, then the factorisation kernel
+  // (each timed on its own when profiling)
+  PhaseTimer ktimer(e);
   auto run_list = [&](const int* list, int count, int N, int form, int slot) {
     const int ch = chunk_targets(N);
     if (count > 0) e.kbuf.reserve(std::max(e.kbuf.bytes, kbuf_bytes(N, std::min(ch, count))));
     for (int c0 = 0; c0 < count; c0 += ch) {
       const int nit = std::min(ch, count - c0);
       KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + slot, 0, sizeof(int), st));
+      ktimer.start();
       launch_assemble(P, N, list, nullptr, c0, nit, e.kbuf.as<double>(), nsm, st);
+      ktimer.stop(4);
+      ktimer.start();
       launch_factor(P, form, N, list, nullptr, c0, nit, e.kbuf.as<double>(), slot, nsm, st);
+      ktimer.stop(5);
       KK_CUDA(cudaGetLastError());
       e.launches += 2;
     }
@@ -828,7 +853,7 @@ void engine_solve(Engine& e) {
       KK_CUDA(cudaGetLastError());
       e.launches += 1;
     } else {
-      run_list(list, count, kernel_rows(ker), refine, slot);
+      run_list(list, count, kernel_rows(ker), kernel_form(ker), slot);
     }
   };
   // ---- kernel per neighbour-count list: fixed, or chosen by timing the
@@ -837,12 +862,12 @@ void engine_solve(Engine& e) {
   int* lists = e.bucket.as<int>();
   for (int li = 0; li < KK_NLIST; ++li) {
     const int count = cb[list_slot(li)];
-    e.plan[li] = count > 0 ? default_kernel(li, wide, e.store_weight != 0) : -1;
+    e.plan[li] = count > 0 ? default_kernel(li, wide, e.store_weight != 0, rform) : -1;
     for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = NAN;
     int cand[KK_NKER];
-    const int nc = candidates(li, wide, e.store_weight != 0, cand);
+    const int nc = candidates(li, wide, e.store_weight != 0, rform, cand);
     if (count <= 0 || nc < 2 || !e.autotune) continue;
-    const TuneKey key = tune_key(P, li, refine, e.st, count);
+    const TuneKey key = tune_key(P, li, rform, e.st, count);
     TuneEntry hit;
     if (e.autotune == 1 && tune_find(key, hit)) {
       e.plan[li] = hit.kernel;
@@ -864,6 +889,15 @@ void engine_solve(Engine& e) {
     };
     e.tunebuf.reserve(sizeof(int) * (size_t)nb);
     KK_CUDA(cudaMemcpyAsync(e.tunebuf.p, P.status, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToDevice, st));
+    // buffers for the largest candidate first: no allocation inside a timing
+    for (int c = 0; c < nc; ++c) {
+      if (cand[c] == KK_KER_GEN) {
+        generic_scratch(ns);
+      } else {
+        const int rows = kernel_rows(cand[c]);
+        e.kbuf.reserve(std::max(e.kbuf.bytes, kbuf_bytes(rows, std::min(chunk_targets(rows), ns))));
+      }
+    }
     const int* l = lists + (size_t)li * nb;
     for (int c = 0; c < nc; ++c) {  // first launches (module loading) outside the timing
       run_kernel(cand[c], l, std::min(ns, 256), KK_CNT_WORK0 + 3);
@@ -875,17 +909,31 @@ void engine_solve(Engine& e) {
     TuneEntry ent;
     ent.kernel = cand[0];
     for (int k = 0; k < KK_NKER; ++k) ent.us[k] = NAN;
-    float best = 0.f;
-    for (int c = 0; c < nc; ++c) {
+    auto timed = [&](int ker, int count) {  // ms of one run on the first count targets
       KK_CUDA(cudaEventRecord(ev[0], st));
-      run_kernel(cand[c], l, ns, KK_CNT_WORK0 + 3);
+      run_kernel(ker, l, count, KK_CNT_WORK0 + 3);
       KK_CUDA(cudaEventRecord(ev[1], st));
       KK_CUDA(cudaEventSynchronize(ev[1]));
       float ms = 0.f;
       KK_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
       restore_counters();
-      ent.us[cand[c]] = 1e3 * ms / ns;
-      if (c == 0 || ms < best) { best = ms; ent.kernel = cand[c]; }
+      return (double)ms;
+    };
+    // a candidate is timed on a quarter of the sample first and dropped there
+    // when it is already more than eight times slower per target than the
+    // best (the general kernel against a register kernel: 27-72x)
+    const int nq = std::max(std::min(ns, 256), ns / 4);
+    double best_us = 0.0;
+    for (int c = 0; c < nc; ++c) {
+      double us;
+      if (c > 0 && nq < ns) {
+        us = 1e3 * timed(cand[c], nq) / nq;
+        if (us <= 8.0 * best_us) us = 1e3 * timed(cand[c], ns) / ns;
+      } else {
+        us = 1e3 * timed(cand[c], ns) / ns;
+      }
+      ent.us[cand[c]] = us;
+      if (c == 0 || us < best_us) { best_us = us; ent.kernel = cand[c]; }
     }
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
@@ -900,10 +948,13 @@ void engine_solve(Engine& e) {
   timer.start();
   for (int li = 0; li < KK_NLIST; ++li) {
     if (e.plan[li] < 0 || e.plan[li] == KK_KER_GEN) continue;
-    run_list(lists + (size_t)li * nb, cb[list_slot(li)], kernel_rows(e.plan[li]), refine, KK_CNT_WORK0 + li);
+    run_list(lists + (size_t)li * nb, cb[list_slot(li)], kernel_rows(e.plan[li]), kernel_form(e.plan[li]),
+             KK_CNT_WORK0 + li);
   }
   timer.stop(2);
-  if (refine) {
+  bool any_r = false;
+  for (int li = 0; li < KK_NLIST; ++li) any_r = any_r || (e.plan[li] >= 0 && kernel_form(e.plan[li]));
+  if (any_r) {
     // targets whose FP32 factorisation failed or whose correction check did
     // not pass: FP64 form (they come from the lists of at most 64 equations)
     int nf = 0;

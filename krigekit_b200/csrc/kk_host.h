@@ -68,7 +68,7 @@ struct Engine {
   int verbose = 0;
   double bounds[2] = {-DBL_MAX, DBL_MAX};
   int st = 0;
-  int precision = 1;   // 0 = FP64 plain, 1 = FP32 factor + FP64 refinement
+  int precision = 2;   // 0 = FP64 plain, 1 = FP32 factor + FP64 refinement, 2 = the faster (tuned)
   int nmin = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -110,7 +110,7 @@ struct Engine {
   // per-phase device time of the last solve (CUDA events on the handle's
   // stream): search, bucket, solve kernels, fallbacks; and kernel launches
   int profile = 0;
-  double phase_ms[4] = {0, 0, 0, 0};
+  double phase_ms[6] = {0, 0, 0, 0, 0, 0};  // [4] assembly, [5] factorisation kernels (inside [2], [3])
   int launches = 0;
   // solve kernel per neighbour-count list (KK_KER_*, -1 for an empty list)
   // in the last solve, and the tuner's measured microseconds per target of

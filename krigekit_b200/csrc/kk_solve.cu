@@ -95,57 +95,92 @@ void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st) {
 // load_block_weights + estimate_block_base (kriging_base.F90:2780-2797,
 // 3407-3503): est_j = sum_v sum_i z_v[inear_v(i)] w_ij, plus the Isaaks &
 // Srivastava shift (std_ck off, several variables), the simple-kriging mean
-// and the bounds.  One warp per target; the lanes take the neighbour rows
-// (weights read coalesced, values gathered), warp sums for the dot products.
-// Targets without neighbours, or marked empty or failed by the solve that
-// filled the store, give NaN.
+// and the bounds.  HBM-bound gather-dot: a group of eight lanes per target,
+// four targets per warp, each lane four neighbour rows per step with every
+// load of the step issued before the first use (weights read contiguously,
+// neighbour indices, then the values gathered from L2); group sums by three
+// shuffles.  Targets without neighbours, or marked empty or failed by the
+// solve that filled the store, give NaN.
+__device__ __forceinline__ double group8_sum(double v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  return v;
+}
+
 __global__ void __launch_bounds__(256) k_replay(const __grid_constant__ SolveParams P) {
-  const int lane = threadIdx.x & 31;
+  constexpr int G = 8, U = 4;  // lanes per target, rows per lane and step
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
   const int q = P.nvar;
   const int nwarp = (gridDim.x * blockDim.x) >> 5;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < P.nblock; t += nwarp) {
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // warp-uniform loop over groups of four targets: every lane reaches every shuffle
+  for (int tb = w0 * 4; tb < P.nblock; tb += nwarp * 4) {
+    const int t = tb + (lane >> 3);
+    const bool valid = t < P.nblock;
     int nn[KK_MAXVAR], ist[KK_MAXVAR], npp = 0;
 #pragma unroll
     for (int v = 0; v < KK_MAXVAR; ++v) {
-      nn[v] = v < q ? __ldg(&P.nnear[v][t]) : 0;
+      nn[v] = (valid && v < q) ? __ldg(&P.nnear[v][t]) : 0;
       ist[v] = npp;
       npp += nn[v];
     }
-    if (npp == 0 || (__ldg(&P.status[t]) & (KK_ST_EMPTY | KK_ST_FAIL))) {
-      if (lane == 0)
-        for (int v = 0; v < q; ++v) P.est[(size_t)t * q + v] = __longlong_as_double(0x7ff8000000000000ll);
-      continue;
-    }
-    double tmean[KK_MAXVAR];
+    const bool nan_out = valid && (npp == 0 || (__ldg(&P.status[t]) & (KK_ST_EMPTY | KK_ST_FAIL)));
+    if (nan_out) npp = 0;
+    // variable loops unrolled to the maximum so nn / ist / tmean stay in registers
+    double tmean[KK_MAXVAR] = {0.0, 0.0, 0.0, 0.0};
     if (P.ck_isa) {
-      for (int v = 0; v < q; ++v) {
+#pragma unroll
+      for (int v = 0; v < KK_MAXVAR; ++v) {
+        if (v >= q) break;
+        const int nv = nan_out ? 0 : nn[v];
+        const int* nb = P.nbr[v] + (size_t)(valid ? t : 0) * P.mmax[v];
         double sz = 0.0;
-        for (int i = lane; i < nn[v]; i += 32)
-          sz += __ldg(&P.oval[v][__ldg(&P.nbr[v][(size_t)t * P.mmax[v] + i])]);
-        sz = warp_sum(sz);
-        tmean[v] = nn[v] > 0 ? sz / nn[v] : 0.0;
+        for (int i = gl; i < nv; i += G) sz += __ldg(&P.oval[v][__ldg(&nb[i])]);
+        sz = group8_sum(sz);
+        tmean[v] = nv > 0 ? sz / nv : 0.0;
       }
     }
-    for (int jv = 0; jv < q; ++jv) {
-      const double* w = P.wout + ((size_t)t * q + jv) * P.wstride;
+#pragma unroll
+    for (int jv = 0; jv < KK_MAXVAR; ++jv) {
+      if (jv >= q) break;
+      const double* w = P.wout + ((size_t)(valid ? t : 0) * q + jv) * P.wstride;
       double avg = 0.0, tws = 0.0;
-      for (int v = 0; v < q; ++v) {
+#pragma unroll
+      for (int v = 0; v < KK_MAXVAR; ++v) {
+        if (v >= q) break;
+        const int nv = nan_out ? 0 : nn[v];
+        const int* nb = P.nbr[v] + (size_t)(valid ? t : 0) * P.mmax[v];
+        const double* z = P.oval[v];
         double dot = 0.0, sw = 0.0;
-        for (int i = lane; i < nn[v]; i += 32) {
-          const double wt = __ldg(&w[ist[v] + i]);
-          dot = fma(__ldg(&P.oval[v][__ldg(&P.nbr[v][(size_t)t * P.mmax[v] + i])]), wt, dot);
-          sw += wt;
+        for (int i0 = 0; i0 < nv; i0 += G * U) {
+          double wt[U];
+          int o[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * G + gl;
+            wt[u] = i < nv ? __ldg(&w[ist[v] + i]) : 0.0;
+            o[u] = i < nv ? __ldg(&nb[i]) : -1;
+          }
+          double zv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) zv[u] = o[u] >= 0 ? __ldg(&z[o[u]]) : 0.0;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            dot = fma(zv[u], wt[u], dot);
+            sw += wt[u];
+          }
         }
-        dot = warp_sum(dot);
-        sw = warp_sum(sw);
+        dot = group8_sum(dot);
+        sw = group8_sum(sw);
         avg += dot;
         tws += sw;
-        if (P.ck_isa && v != jv && nn[v] > 0) avg += (tmean[jv] - tmean[v]) * sw;
+        if (P.ck_isa && v != jv && nv > 0) avg += (tmean[jv] - tmean[v]) * sw;
       }
       if (P.unbias == 0 && P.sk_mean[jv] != 0.0) avg += (1.0 - tws) * P.sk_mean[jv];
       if (avg < P.bounds[0]) avg = P.bounds[0];
       if (avg > P.bounds[1]) avg = P.bounds[1];
-      if (lane == 0) P.est[(size_t)t * q + jv] = avg;
+      if (valid && gl == 0) P.est[(size_t)t * q + jv] = nan_out ? __longlong_as_double(0x7ff8000000000000ll) : avg;
     }
   }
 }
@@ -174,7 +209,7 @@ void launch_indicator_post(double* est, int nb, int nvar, int kcat, int nsm, cud
 }
 
 void launch_replay(const SolveParams& P, int nsm, cudaStream_t st) {
-  const int need = (P.nblock + 7) / 8;  // eight warps per block
+  const int need = (P.nblock + 31) / 32;  // eight warps of four targets per block
   const int blocks = std::max(1, std::min(need, nsm * 8));
   k_replay<<<blocks, 256, 0, st>>>(P);
 }

@@ -7,9 +7,10 @@ Mirrors the reference wrapper ougx/krigekit src/krigekit/kriging.py
 C call, and the same result arrays / DataFrame columns.  Every call goes to
 ``libkrigecuda.so`` (sm_100a); there is no CPU path.
 
-GPU-specific keyword extensions: ``precision`` ("fp32_refine" = FP32
-factorisation with FP64 iterative refinement, or "fp64"), ``nmin``
-(targets with fewer neighbours give NaN), ``device``.
+GPU-specific keyword extensions: ``precision`` ("auto" = per neighbour-count
+list the faster of the two forms as timed by the kernel tuner, FP64 when not
+tuned; "fp32_refine" = FP32 factorisation with an FP64 residual correction;
+"fp64"), ``nmin`` (targets with fewer neighbours give NaN), ``device``.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ from . import _lib
 
 _c_int = ctypes.c_int
 _c_double = ctypes.c_double
-_PRECISION = {"fp64": 0, "fp32_refine": 1}
+_PRECISION = {"fp64": 0, "fp32_refine": 1, "auto": 2}
 
 
 def _farray(a, dtype=np.float64):
@@ -56,21 +57,22 @@ def _iptr(a):
 
 
 
-KERNELS = ("warp32", "warp64", "block128", "general")
+KERNELS = ("warp32", "warp64", "block128", "general", "warp32_fp32r", "warp64_fp32r")
 PLAN_LISTS = ("npp<=32", "npp<=64", "npp>128", "npp<=128")
 
 
 def kernel_plan(handle) -> dict:
     """{list: {"kernel": name, "us_per_target": {candidate: us}}} of the last
     solve of a handle (krige_get_kernel_plan); empty lists are left out."""
+    nk = len(KERNELS)
     ker = (ctypes.c_int * 4)()
-    us = (ctypes.c_double * 16)()
+    us = (ctypes.c_double * (4 * nk))()
     _lib.call("krige_get_kernel_plan", handle, ker, us)
     out = {}
     for li, name in enumerate(PLAN_LISTS):
         if ker[li] < 0:
             continue
-        timed = {KERNELS[k]: us[li * 4 + k] for k in range(4) if us[li * 4 + k] == us[li * 4 + k]}
+        timed = {KERNELS[k]: us[li * nk + k] for k in range(nk) if us[li * nk + k] == us[li * nk + k]}
         out[name] = {"kernel": KERNELS[ker[li]], "us_per_target": timed}
     return out
 
@@ -101,7 +103,7 @@ class Kriging:
         weight_file: str = "",
         bounds: Optional[tuple] = None,
         seed: Optional[int] = None,
-        precision: str = "fp32_refine",
+        precision: str = "auto",
         nmin: int = 0,
         device: Optional[int] = None,
     ):
@@ -342,8 +344,10 @@ class Kriging:
         out = (ctypes.c_double * 4)()
         nl = ctypes.c_int(0)
         _lib.call("krige_gpu_phases", self._h(), out, ctypes.byref(nl))
+        km = (ctypes.c_double * 2)()
+        _lib.call("krige_gpu_kernel_ms", self._h(), km)
         return {"search_ms": out[0], "bucket_ms": out[1], "solve_ms": out[2], "fallback_ms": out[3],
-                "launches": nl.value}
+                "assemble_ms": km[0], "factor_ms": km[1], "launches": nl.value}
 
     # ------------------------------------------------------------------ results
     def _nb(self):

@@ -70,7 +70,7 @@ class SpaceTimeKriging:
         weight_file: str = "",
         bounds: Optional[tuple] = None,
         seed: Optional[int] = None,
-        precision: str = "fp32_refine",
+        precision: str = "auto",
         nmin: int = 0,
         device: Optional[int] = None,
     ):
@@ -284,8 +284,10 @@ class SpaceTimeKriging:
         out = (ctypes.c_double * 4)()
         nl = ctypes.c_int(0)
         _lib.call("krige_gpu_phases", self._h(), out, ctypes.byref(nl))
+        km = (ctypes.c_double * 2)()
+        _lib.call("krige_gpu_kernel_ms", self._h(), km)
         return {"search_ms": out[0], "bucket_ms": out[1], "solve_ms": out[2], "fallback_ms": out[3],
-                "launches": nl.value}
+                "assemble_ms": km[0], "factor_ms": km[1], "launches": nl.value}
 
     # ------------------------------------------------------------------ results
     def _nb(self):

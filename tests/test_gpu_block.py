@@ -156,35 +156,42 @@ def test_ragged_sizes_fill_every_list():
         assert c["bucket_le128"] == ((npp > 64) & (npp <= 128)).sum() > 0
         assert c["bucket_gt128"] == (npp > 128).sum() > 0
         plan = g.kernel_plan()
+        sfx = "" if precision == "fp64" else "_fp32r"
         assert [plan[k]["kernel"] for k in ("npp<=32", "npp<=64", "npp<=128", "npp>128")] == \
-            ["warp32", "warp64", "block128", "general"]
+            ["warp32" + sfx, "warp64" + sfx, "block128", "general"]
 
 
 def test_autotune_times_candidates_and_leaves_no_trace():
-    """autotune=2 times both candidates of each list long enough to tune on a
-    sample and keeps the faster; the sample runs must not show in the
+    """autotune=2 times the candidates of each list long enough to tune on a
+    sample (both forms of each warp kernel under precision "auto") and keeps
+    the fastest; the sample runs must not show in the
     counters, the status bits or the results (the chosen kernel solves the
     whole list afterwards)."""
     rng = np.random.default_rng(33)
     x = rng.uniform(0, 1, (6000, 2))
     z = bw.cosine_field(rng, 2, 0.2)(x) + rng.normal(0, 0.05, len(x))
     grid = rng.uniform(0, 1, (2600, 2))
-    for nmax, lst, cands in ((24, "npp<=32", {"warp32", "warp64"}), (48, "npp<=64", {"warp64", "block128"}),
-                             (80, "npp<=128", {"block128", "general"})):
+    cands = {("npp<=32", "fp64"): {"warp32", "warp64"},
+             ("npp<=32", "fp32_refine"): {"warp32_fp32r", "warp64_fp32r"},
+             ("npp<=32", "auto"): {"warp32", "warp32_fp32r", "warp64", "warp64_fp32r"},
+             ("npp<=64", "fp64"): {"warp64", "block128"},
+             ("npp<=64", "fp32_refine"): {"warp64_fp32r", "block128"},
+             ("npp<=64", "auto"): {"warp64", "warp64_fp32r", "block128"}}
+    for nmax, lst in ((24, "npp<=32"), (48, "npp<=64"), (80, "npp<=128")):
         w = dict(ndim=2, nvar=1, kw={}, obs=[dict(coord=x, value=z, nmax=nmax)],
                  vgm=[(1, 1, dict(vtype="sph", nugget=0.02, sill=1.0, a_major=0.25))], search=[dict()],
                  grid=grid, zstd=float(np.std(z)), sill=1.02)
-        for precision in ("fp64", "fp32_refine"):
+        for precision in ("fp64", "fp32_refine", "auto"):
             g, o = _run(w, precision, autotune=2)
             plan = g.kernel_plan()[lst]
-            assert set(plan["us_per_target"]) == cands, plan
+            assert set(plan["us_per_target"]) == cands.get((lst, precision), {"block128", "general"}), plan
             assert plan["kernel"] == min(plan["us_per_target"], key=plan["us_per_target"].get)
             c = g.gpu_counters()
             assert c["chol"] == len(grid) and c["fail"] == 0 and c["ldlt"] == 0, c
             st = g.get_status()
             assert int(((st & 4) != 0).sum()) == c["fp64_resolve"]
             assert not (st & 8).any()
-            if precision == "fp64" or plan["kernel"] in ("block128", "general"):
+            if not plan["kernel"].endswith("_fp32r"):
                 _compare(g, o, w)
             else:
                 e, _ = g.get_results()
