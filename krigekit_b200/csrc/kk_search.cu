@@ -708,18 +708,31 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       if (d < g.G) c[d] = cell_coord(g, d, qg[d]);
-    int R = 0;
-    for (;; ++R) {
+    // the smallest ring R whose box is the whole grid or holds K + 1 points
+    // (both monotone in R): lane l tests R0 + l, 32 rings per round trip
+    int R = -1;
+    for (int R0 = 0; R < 0; R0 += 32) {
+      const int Rl = R0 + lane;
       bool full = true;
+      int al[3] = {0, 0, 0}, bl[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         if (d < g.G) {
-          a[d] = max(0, c[d] - R);
-          bb[d] = min(g.n[d] - 1, c[d] + R);
-          if (a[d] > 0 || bb[d] < g.n[d] - 1) full = false;
+          al[d] = max(0, c[d] - Rl);
+          bl[d] = min(g.n[d] - 1, c[d] + Rl);
+          if (al[d] > 0 || bl[d] < g.n[d] - 1) full = false;
         }
       }
-      if (full || box_count(g, a, bb) >= (long long)K + 1) break;
+      const bool ok = full || box_count(g, al, bl) >= (long long)K + 1;
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (m) R = R0 + __ffs(m) - 1;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d < g.G) {
+        a[d] = max(0, c[d] - R);
+        bb[d] = min(g.n[d] - 1, c[d] + R);
+      }
     }
     // farthest corner of the box (every search dimension), with a margin
     double D2 = 0.0;
@@ -820,36 +833,48 @@ __global__ void __launch_bounds__(128) k_search(KkSearch S, int ntarget, const d
         rstart[lane] = incl - len;
         rp0[lane] = p0;
         __syncwarp();
-        for (int base = 0; base < tot; base += 32) {
-          const int i = base + lane;
-          int j = 0;
-          double d2v = 0.0;
-          bool in = false;
-          if (i < tot) {
-            int k = 0;
+        // two batches of 32 per round: every global load of both (coordinates,
+        // original index) is issued before the first ballot
+        for (int base = 0; base < tot; base += 64) {
+          double d2v[2] = {0.0, 0.0};
+          int oi[2] = {0, 0}, sec[2] = {0, 0};
+          bool in[2] = {false, false};
 #pragma unroll
-            for (int step = 16; step > 0; step >>= 1)
-              if (rstart[k + step] <= i) k += step;
-            j = rp0[k] + (i - rstart[k]);
-            d2v = dist2(g, q, j);
-            in = d2v <= D2;
-          }
-          unsigned m = __ballot_sync(0xffffffffu, in);
-          int pos = M + __popc(m & lanemask_lt());
-          if (in && pos < CAP) {
-            int oi = __ldg(&g.sidx[j]);
-            B.d2[pos] = d2v;
-            B.idx[pos] = oi;
-            if (S.mode == 2) {
-              double dx = dsub(__ldg(&g.sc[j]), q[0]);
-              double dy = S.ndim > 1 ? dsub(__ldg(&g.sc[(size_t)g.nobs + j]), q[1]) : 0.0;
-              double dz = S.ndim == 3 ? dsub(__ldg(&g.sc[(size_t)2 * g.nobs + j]), q[2]) : 0.0;
-              int sec = (dx < 0.0 ? 1 : 0) + (dy < 0.0 ? 2 : 0) + (dz < 0.0 ? 4 : 0);
-              B.sec[pos] = (signed char)sec;
+          for (int u = 0; u < 2; ++u) {
+            const int i = base + 32 * u + lane;
+            if (i < tot) {
+              int k = 0;
+#pragma unroll
+              for (int step = 16; step > 0; step >>= 1)
+                if (rstart[k + step] <= i) k += step;
+              const int j = rp0[k] + (i - rstart[k]);
+              // dist2 with the sector signs of the same differences
+              double sd = 0.0;
+#pragma unroll
+              for (int d = 0; d < 4; ++d) {
+                if (d < g.D) {
+                  const double t = dsub(__ldg(&g.sc[(size_t)d * g.nobs + j]), q[d]);
+                  sd = dadd(sd, dmul(t, t));
+                  if (d < S.ndim && t < 0.0) sec[u] += 1 << d;
+                }
+              }
+              d2v[u] = sd;
+              in[u] = sd <= D2;
+              oi[u] = __ldg(&g.sidx[j]);
             }
           }
-          M += __popc(m);
-          if (M > CAP) overflow = true;
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const unsigned m = __ballot_sync(0xffffffffu, in[u]);
+            const int pos = M + __popc(m & lanemask_lt());
+            if (in[u] && pos < CAP) {
+              B.d2[pos] = d2v[u];
+              B.idx[pos] = oi[u];
+              if (S.mode == 2) B.sec[pos] = (signed char)sec[u];
+            }
+            M += __popc(m);
+            if (M > CAP) overflow = true;
+          }
         }
         __syncwarp();  // the next group reuses rstart / rp0
       }
