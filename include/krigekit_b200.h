@@ -120,8 +120,15 @@ int krige_get_nblocks(int64_t handle, int *nblocks);
 int krige_get_nsim(int64_t handle, int *nsim);
 /* kriging_capi_common.F90:277-288 krige_get_block_coord: out(ndim_c, nblocks). */
 int krige_get_block_coord(int64_t handle, int ndim_c, int nblocks, double *out);
-/* kriging_capi_common.F90:290-306 krige_get_estimate: out(nblocks, nsim_c), variable 1. */
+/* kriging_capi_common.F90:290-306 krige_get_estimate: out(nblocks, nsim_c), variable 1
+ * (the realisations of a sequential simulation when nsim > 0). */
 int krige_get_estimate(int64_t handle, int nsim_c, int nblocks, double *out);
+/* kriging_capi.F90:410-443 krige_set_sim: SGSIM visiting order randpath(nblocks), 1-based,
+ * and N(0, 1) draws sample(nsim_c, nvar_c, nblocks) of the p-th visited target; either
+ * pointer may be NULL (a seeded random order / draws, not the reference's generator).
+ * One variable, point targets, no sector search or external drift. */
+int krige_set_sim(int64_t handle, int nblocks, const int *randpath, int nsim_c, int nvar_c,
+                  const double *sample);
 /* kriging_capi_common.F90:323-344 krige_get_estimate_all: out(nblocks, nvar_c, nsim_c). */
 int krige_get_estimate_all(int64_t handle, int nblocks, int nvar_c, int nsim_c, double *out);
 /* kriging_capi_common.F90:352-369 krige_get_variance: out(nblocks), variable 1. */

@@ -14,7 +14,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libkrigecuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kk_search.cu", "kk_solve.cu", "kk_engine.cu"]
+CU_SOURCES = ["kk_search.cu", "kk_solve.cu", "kk_engine.cu", "kk_sgsim.cu"]
 CPP_SOURCES = ["kk_host.cpp", "kk_capi.cpp"]
 HEADERS = ["kk_common.h", "kk_device.cuh", "kk_host.h", "kk_kernels.h", "kk_warp.cuh", "kk_block.cuh",
            "kk_solve_common.cuh"]

@@ -242,7 +242,8 @@ __global__ void __launch_bounds__(128, 2)
           s.G[kb * C + ka] = g;
         }
       int f = 0;
-      finish_outputs(P, t, s.G, C, s.zmean, &f);
+      if (C == 3 && P.pa == 1 && q == 1) finish_ok(P, t, s.G, &f);
+      else finish_outputs(P, t, s.G, C, s.zmean, &f);
       if (f) {
         P.status[t] |= KK_ST_LDLT;
         const int p = atomicAdd(&P.counters[KK_CNT_FB], 1);

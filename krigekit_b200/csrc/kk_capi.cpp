@@ -163,11 +163,12 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
                      int weight_correction, int use_old_weight, int store_weight, int cross_validation,
                      int write_mat, int neglect_error, int varying_vgm, int std_ck, int verbose, int pf_cache,
                      const char* weight_file, const double* bounds, int seed) {
-  (void)pf_cache; (void)weight_file; (void)seed; (void)write_mat;
+  (void)pf_cache; (void)weight_file; (void)write_mat;
   KK_GUARD_BEGIN
   Engine* e = get(h);
   if (!e) return 1;
-  if (nsim > 0) throw std::string("sequential simulation (nsim > 0) is not part of the GPU kriging path");
+  if (nsim < 0) throw std::string("nsim must be >= 0");
+  if (nsim > 0 && cross_validation) throw std::string("cross_validation and nsim>0 are mutually exclusive");
   if (store_weight && use_old_weight) throw std::string("store_weight and use_old_weight are mutually exclusive");
   if ((store_weight || use_old_weight) && weight_file && weight_file[0])
     throw std::string("weight files are not written by the GPU library: keep the weight store in memory "
@@ -200,6 +201,9 @@ int krige_initialize(int64_t h, int ndim, int nvar, int ndrift, int unbias, int 
   e->ndrift = ndrift;
   e->unbias = unbias;
   e->nsim = nsim;
+  e->seed = seed;
+  e->sim_path.clear();
+  e->sim_sample.clear();
   e->anisotropic_search = anisotropic_search;
   e->cross_validation = cross_validation;
   e->neglect_error = neglect_error;
@@ -582,7 +586,7 @@ int krige_get_nsim(int64_t h, int* ns) {
   KK_GUARD_BEGIN
   Engine* e = get(h);
   if (!e) return 1;
-  *ns = 0;
+  *ns = e->nsim;
   KK_GUARD_END
 }
 
@@ -615,6 +619,15 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
   if (nblocks < 0 || nblocks > e->nblock || nvar_c < 0 || nvar_c > nv || nsim_c < 0)
     throw std::string("output dimensions exceed the solved blocks or variables");
   if (nblocks == 0 || nvar_c == 0 || nsim_c == 0) return 0;
+  if (e->nsim > 0) {
+    // sequential simulation: est is (nblock, nsim) on the device, one variable
+    if (nsim_c > e->nsim) throw std::string("nsim exceeds the simulated realisations");
+    std::vector<double> fb;
+    const double* tmp = results_to_host(e, e->est.p, (size_t)e->nblock * e->nsim, fb);
+    for (int is = 0; is < nsim_c; ++is)
+      for (int ib = 0; ib < nblocks; ++ib) out[ib + (size_t)nblocks * nvar_c * is] = tmp[(size_t)ib * e->nsim + is];
+    return 0;
+  }
   if (nv == 1) {
     // est is (nblock) on the device: copy the first column straight into out
     copy_d2h(out, e->est.p, sizeof(double) * nblocks);
@@ -633,6 +646,44 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
 // krige_get_estimate, kriging_capi_common.F90:290-306: out(nblocks, nsim) of variable 1
 int krige_get_estimate(int64_t h, int nsim_c, int nblocks, double* out) {
   return krige_get_estimate_all(h, nblocks, 1, nsim_c, out);
+}
+
+// krige_set_sim, kriging_capi.F90:410-443 -> set_sim_base (kriging_base.F90:1226-1320):
+// randpath (nblocks, 1-based) and sample (nsim, nvar, nblocks), either may be NULL
+int krige_set_sim(int64_t h, int nblocks, const int* randpath, int nsim_c, int nvar_c, const double* sample) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (e->nsim == 0) return 0;
+  if (e->obs.empty()) throw std::string("call initialize() before set_sim().");
+  if (e->nblock == 0) throw std::string("Grid needs to be set first.");
+  for (const ObsVar& o : e->obs)
+    if (o.n == 0) throw std::string("Observations need to be set first.");
+  for (const ObsVar& o : e->obs)
+    if (o.nmax > (int)(INT_MAX * 0.001)) throw std::string("`nmax` must be set for all observations for SGSIM.");
+  const int nb = e->nblock;
+  if (randpath) {
+    if (nblocks != nb) throw std::string("size(randpath) /= nblock");
+    std::vector<char> seen(nb, 0);
+    for (int i = 0; i < nb; ++i) {
+      if (randpath[i] < 1 || randpath[i] > nb || seen[randpath[i] - 1])
+        throw std::string("randpath must be a 1-based permutation of 1..nblocks");
+      seen[randpath[i] - 1] = 1;
+    }
+    e->sim_path.assign(randpath, randpath + nb);
+  } else {
+    engine_sim_defaults(*e, true, false);
+  }
+  if (sample) {
+    if (nsim_c != e->nsim) throw std::string("size(sample, 1) /= nsim");
+    if (nvar_c != e->nvar) throw std::string("size(sample, 2) /= nvar");
+    if (nblocks != nb) throw std::string("size(sample, 3) /= nblock");
+    e->sim_sample.assign(sample, sample + (size_t)nsim_c * nvar_c * nb);
+  } else {
+    engine_sim_defaults(*e, false, true);
+  }
+  e->solved = false;
+  KK_GUARD_END
 }
 
 // krige_get_variance_all, kriging_capi_common.F90:372-392: out(nblocks, nvar, nvar)

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -512,7 +513,13 @@ void tune_clear() {
 
 static void engine_replay(Engine& e);
 
+static void engine_sgsim(Engine& e);
+
 void engine_solve(Engine& e) {
+  if (e.nsim > 0) {
+    engine_sgsim(e);
+    return;
+  }
   auto t0 = std::chrono::steady_clock::now();
   for (double& x : e.phase_ms) x = 0.0;
   e.launches = 0;
@@ -667,6 +674,23 @@ void engine_solve(Engine& e) {
     mm_total += S.mmax;
     const double* tx[4] = {e.tx[0].as<double>(), e.tx[1].as<double>(), e.tx[2].as<double>(), e.tx[3].as<double>()};
     const double* ox[4] = {d.x[0].as<double>(), d.x[1].as<double>(), d.x[2].as<double>(), d.x[3].as<double>()};
+    if (e.sim_nobs >= 0) {
+      // the systems of a sequential simulation: every target searches the
+      // observations and the targets visited before it (exact kd-tree order)
+      if (S.mode != 0 && !d.tree_ready) build_tree(e, v);
+      const int nthreads = std::max(1, std::min(nb, 32768));
+      const int stride = S.nmax + 2;
+      DBuf heaps;
+      heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);
+      timer.start();
+      launch_search_sgsim(S, nb, e.sim_nobs, tx, ox, d.nbr.as<int>(), d.nnear.as<int>(), heaps.p, stride,
+                          nthreads, st);
+      KK_CUDA(cudaGetLastError());
+      timer.stop(0);
+      e.launches += 1;
+      KK_CUDA(cudaStreamSynchronize(st));
+      continue;
+    }
     KK_CUDA(cudaMemsetAsync(e.counters.as<int>() + KK_CNT_REDO + v, 0, sizeof(int), st));
     timer.start();
     launch_search(S, nb, tx, ox, d.nbr.as<int>(), d.nnear.as<int>(), e.status.as<int>(), redo,
@@ -820,8 +844,14 @@ void engine_solve(Engine& e) {
   const int rform = (e.store_weight || !solve_refine_form(P, e.precision)) ? 0 : e.precision;
   const int mtot = mm_total + P.pa;
   const size_t gstride = generic_stride(mtot, nv, P.pa);
+  // threads of the general kernel for a list of count targets: one target
+  // each at a time, as many as a 4 GiB workspace holds (at least 2 048, a
+  // multiple of 64, at most 65 536)
+  const int gen_cap = (int)std::max<size_t>(
+      2048, std::min<size_t>(65536, ((size_t)4 << 30) / (sizeof(double) * gstride)) / 64 * 64);
+  auto gen_threads = [&](int count) { return std::max(1, std::min(count, gen_cap)); };
   auto generic_scratch = [&](int nthreads) {
-    e.scratch.reserve(sizeof(double) * gstride * std::max(1, std::min(nthreads, 2048)));
+    e.scratch.reserve(sizeof(double) * gstride * gen_threads(nthreads));
     P.scratch = e.scratch.as<double>();
     P.scratch_stride = (int)gstride;
   };
@@ -849,7 +879,7 @@ void engine_solve(Engine& e) {
     if (ker == KK_KER_GEN) {
       generic_scratch(count);
       KK_CUDA(cudaMemcpyAsync(e.counters.as<int>() + KK_CNT_TUNE, &count, sizeof(int), cudaMemcpyHostToDevice, st));
-      launch_solve_generic(P, list, KK_CNT_TUNE, std::min(count, 2048), st);
+      launch_solve_generic(P, list, KK_CNT_TUNE, gen_threads(count), st);
       KK_CUDA(cudaGetLastError());
       e.launches += 1;
     } else {
@@ -980,11 +1010,11 @@ void engine_solve(Engine& e) {
     for (int li = 0; li < KK_NLIST; ++li) {
       const int c = cnt[list_slot(li)];
       if (e.plan[li] != KK_KER_GEN || c <= 0) continue;
-      launch_solve_generic(P, lists + (size_t)li * nb, list_slot(li), std::min(c, 2048), st);
+      launch_solve_generic(P, lists + (size_t)li * nb, list_slot(li), gen_threads(c), st);
       e.launches += 1;
     }
     if (cnt[KK_CNT_FB] > 0) {
-      launch_solve_generic(P, P.fb_list, KK_CNT_FB, std::min(cnt[KK_CNT_FB], 2048), st);
+      launch_solve_generic(P, P.fb_list, KK_CNT_FB, gen_threads(cnt[KK_CNT_FB]), st);
       e.launches += 1;
     }
     KK_CUDA(cudaGetLastError());
@@ -1278,6 +1308,206 @@ void engine_free_weight_store(Engine& e) {
   e.use_old_weight = 0;
 }
 
+// ---------------------------------------------------------------------------
+// sequential Gaussian simulation (nsim > 0)
+// ---------------------------------------------------------------------------
+// set_sim_base without a path or samples (kriging_base.F90:1255-1300): a
+// random visiting order and N(0, 1) draws.  The reference draws them with its
+// own generator and writes them to sgs_path.dat / sgs_sample.dat; here they
+// come from a 64-bit Mersenne twister seeded by initialize's seed (a random
+// seed when it is 0) and stay in memory, so a given seed repeats its
+// realisations but does not repeat the reference's.
+void engine_sim_defaults(Engine& e, bool path, bool sample) {
+  const int nb = e.nblock;
+  std::mt19937_64 rng(e.seed != 0 ? (uint64_t)(int64_t)e.seed : (uint64_t)std::random_device{}());
+  if (path) {
+    e.sim_path.resize(nb);
+    for (int i = 0; i < nb; ++i) e.sim_path[i] = i + 1;
+    std::shuffle(e.sim_path.begin(), e.sim_path.end(), rng);
+  }
+  if (sample) {
+    std::normal_distribution<double> nd(0.0, 1.0);
+    e.sim_sample.resize((size_t)nb * e.nsim * e.nvar);
+    for (auto& x : e.sim_sample) x = nd(rng);
+  }
+}
+
+// The simulation (solve_base with nsim > 0, kriging_base.F90:2055-2181): an
+// internal engine holds the observations followed by the targets in visiting
+// order and solves every target's system at once, with the search limited to
+// the observations and the targets visited before it and the weights kept;
+// then the values are drawn level by level (k_sgsim_level).
+static void engine_sgsim(Engine& e) {
+  auto t0 = std::chrono::steady_clock::now();
+  for (double& x : e.phase_ms) x = 0.0;
+  e.launches = 0;
+  if (e.nvar != 1)
+    throw std::string("sequential simulation of several variables (joint co-simulation) is not supported by the "
+                      "GPU library; simulate one variable");
+  if (e.st) throw std::string("space-time sequential simulation is not supported by the GPU library");
+  if (!e.nblockpnt.empty()) throw std::string("sequential simulation needs point targets (set_grid)");
+  if (e.ndrift > 0) throw std::string("sequential simulation with external drift is not supported by the GPU library");
+  if (e.store_weight || e.use_old_weight) throw std::string("the weight store is not used with sequential simulation");
+  if (e.obs.empty() || e.obs[0].n == 0) throw std::string("Observations need to be set first.");
+  if (e.nblock == 0) throw std::string("Grid needs to be set first.");
+  ObsVar& o = e.obs[0];
+  if (o.sector) throw std::string("sector search in sequential simulation is not supported by the GPU library");
+  if (o.nmax > (int)(INT_MAX * 0.001)) throw std::string("`nmax` must be set for all observations for SGSIM.");
+  validate(e);
+  const int nb = e.nblock, D = e.nlag, nsim = e.nsim, nobs = o.n;
+  if ((int)e.sim_path.size() != nb) engine_sim_defaults(e, true, false);
+  if (e.sim_sample.size() != (size_t)nb * nsim) engine_sim_defaults(e, false, true);
+  {
+    std::vector<char> seen(nb, 0);
+    for (int p = 0; p < nb; ++p) {
+      const int t = e.sim_path[p];
+      if (t < 1 || t > nb || seen[t - 1]) throw std::string("randpath must be a 1-based permutation of 1..nblocks");
+      seen[t - 1] = 1;
+    }
+  }
+  const double* bc = e.bcoord_staged ? static_cast<const double*>(e.hstage) : e.bcoord.data();
+  cudaStream_t st = e.stream;
+  KK_CUDA(cudaSetDevice(e.device));
+  const int nsm = sm_count(e.device);
+
+  // ---- the systems: observations + targets in visiting order, weights kept
+  Engine s;
+  struct Release {
+    Engine& x;
+    ~Release() { engine_release(x); }
+  } release{s};
+  s.ndim = e.ndim;
+  s.nlag = e.nlag;
+  s.nvar = 1;
+  s.ndrift = 0;
+  s.unbias = e.unbias;
+  s.anisotropic_search = e.anisotropic_search;
+  s.neglect_error = e.neglect_error;
+  s.std_ck = e.std_ck;
+  s.precision = 0;
+  s.nmin = e.nmin;
+  s.device = e.device;
+  s.stream = e.stream;
+  s.autotune = e.autotune;
+  s.profile = e.profile;
+  s.store_weight = 1;
+  s.sim_nobs = nobs;
+  s.obs.assign(1, o);
+  ObsVar& so = s.obs[0];
+  so.n = nobs + nb;
+  so.coord.resize((size_t)D * so.n);
+  for (int p = 0; p < nb; ++p)
+    for (int k = 0; k < D; ++k) so.coord[(size_t)(nobs + p) * D + k] = bc[(size_t)(e.sim_path[p] - 1) * D + k];
+  so.value.resize(so.n, 0.0);
+  so.variance.resize(so.n, 0.0);  // simulated targets carry no measurement error
+  so.dirty = true;
+  so.search_dirty = true;
+  s.vgm[0][0] = e.vgm[0][0];
+  s.nblock = nb;
+  s.bcoord.resize((size_t)D * nb);
+  for (int p = 0; p < nb; ++p)
+    for (int k = 0; k < D; ++k) s.bcoord[(size_t)p * D + k] = bc[(size_t)(e.sim_path[p] - 1) * D + k];
+  if (!e.rangescale.empty()) {
+    s.rangescale.resize(nb);
+    for (int p = 0; p < nb; ++p) s.rangescale[p] = e.rangescale[e.sim_path[p] - 1];
+  }
+  if (!e.localnugget.empty()) {
+    s.localnugget.resize(nb);
+    for (int p = 0; p < nb; ++p) s.localnugget[p] = e.localnugget[e.sim_path[p] - 1];
+  }
+  s.grid_dirty = true;
+  engine_solve(s);
+
+  // ---- dependency levels: one above the highest level among the target's
+  // simulated neighbours (all visited before it, so one pass in visiting order)
+  const int mm = std::max(s.vd[0].search.mmax, 1);
+  std::vector<int> hn(nb), hl((size_t)nb * mm);
+  KK_CUDA(cudaMemcpyAsync(hn.data(), s.vd[0].nnear.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaMemcpyAsync(hl.data(), s.vd[0].nbr.p, sizeof(int) * hl.size(), cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> lev(nb, 0);
+  int nlev = 0;
+  for (int p = 0; p < nb; ++p) {
+    int L = 0;
+    for (int i = 0; i < hn[p]; ++i) {
+      const int idx = hl[(size_t)p * mm + i];
+      if (idx >= nobs) L = std::max(L, lev[idx - nobs] + 1);
+    }
+    lev[p] = L;
+    nlev = std::max(nlev, L + 1);
+  }
+  std::vector<int> off((size_t)nlev + 1, 0), order(nb);
+  for (int p = 0; p < nb; ++p) off[lev[p] + 1]++;
+  for (int L = 0; L < nlev; ++L) off[L + 1] += off[L];
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int p = 0; p < nb; ++p) order[fill[lev[p]]++] = p;
+  }
+
+  // ---- the draws, level by level
+  DBuf dorder, dpath, dsample, dsim;
+  upload(dorder, order.data(), sizeof(int) * nb, st);
+  upload(dpath, e.sim_path.data(), sizeof(int) * nb, st);
+  upload(dsample, e.sim_sample.data(), sizeof(double) * e.sim_sample.size(), st);
+  dsim.reserve(sizeof(double) * (size_t)nsim * nb);
+  e.est.reserve(sizeof(double) * (size_t)nb * nsim);
+  e.var.reserve(sizeof(double) * nb);
+  e.status.reserve(sizeof(int) * nb);
+  SimParams SP;
+  SP.nbr = s.vd[0].nbr.as<int>();
+  SP.nnear = s.vd[0].nnear.as<int>();
+  SP.w = s.wbuf.as<double>();
+  SP.var = s.var.as<double>();
+  SP.z = s.vd[0].value.as<double>();
+  SP.sample = dsample.as<double>();
+  SP.path = dpath.as<int>();
+  SP.sim = dsim.as<double>();
+  SP.out = e.est.as<double>();
+  SP.nb = nb;
+  SP.nobs = nobs;
+  SP.nsim = nsim;
+  SP.mmax = mm;
+  SP.wstride = s.wstride;
+  SP.sk = e.unbias == 0 ? 1 : 0;
+  SP.sk_mean = o.sk_mean;
+  SP.lo = e.bounds[0];
+  SP.hi = e.bounds[1];
+  PhaseTimer timer(e);
+  timer.start();
+  for (int L = 0; L < nlev; ++L) {
+    launch_sgsim_level(SP, dorder.as<int>() + off[L], off[L + 1] - off[L], nsm, st);
+    KK_CUDA(cudaGetLastError());
+  }
+  timer.stop(2);
+
+  // ---- variance and status in target order
+  std::vector<double> hv(nb), tv(nb);
+  std::vector<int> hs(nb), ts(nb);
+  KK_CUDA(cudaMemcpyAsync(hv.data(), s.var.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaMemcpyAsync(hs.data(), s.status.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+  KK_CUDA(cudaStreamSynchronize(st));
+  for (int p = 0; p < nb; ++p) {
+    tv[e.sim_path[p] - 1] = hv[p];
+    ts[e.sim_path[p] - 1] = hs[p];
+  }
+  upload(e.var, tv.data(), sizeof(double) * nb, st);
+  upload(e.status, ts.data(), sizeof(int) * nb, st);
+  KK_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 4; ++i) e.phase_ms[i] += s.phase_ms[i];
+  e.phase_ms[4] = s.phase_ms[4];
+  e.phase_ms[5] = s.phase_ms[5];
+  e.launches += s.launches + nlev;
+  std::memcpy(e.stats, s.stats, sizeof e.stats);
+  std::memcpy(e.counters_last, s.counters_last, sizeof e.counters_last);
+  for (int li = 0; li < KK_NLIST; ++li) {
+    e.plan[li] = s.plan[li];
+    for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = s.plan_us[li][k];
+  }
+  e.sim_levels = nlev;
+  e.mmax_total = mm;
+  e.solved = true;
+  e.last_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 void engine_release(Engine& e) {
   for (int v = 0; v < KK_MAXVAR; ++v) {
     VarDevice& d = e.vd[v];

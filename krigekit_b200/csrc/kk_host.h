@@ -142,6 +142,17 @@ struct Engine {
   int wh_nm = 0;
   std::string info;               // krige_to_str text
 
+  // sequential simulation (nsim > 0, krige_set_sim): visiting order (1-based
+  // targets) and N(0, 1) draws sample[p * nsim + s] of the p-th visited
+  // target; generated from seed when not given.  sim_nobs >= 0 marks the
+  // internal engine that solves the simulation's systems: its observations
+  // are the sim_nobs data followed by the targets in visiting order.
+  int seed = 0;
+  std::vector<int> sim_path;
+  std::vector<double> sim_sample;
+  int sim_nobs = -1;
+  int sim_levels = 0;  // dependency levels of the last simulation
+
   int naug() const { return std_ck ? unbias * nvar : unbias; }
   int pdrift() const { return ndrift + naug(); }
 };
@@ -156,6 +167,9 @@ void build_kdtree(const double* data, int D, int n, std::vector<int>& node_i,
 
 // engine entry points (kk_engine.cu)
 void engine_solve(Engine& e);
+// visiting order and draws of a sequential simulation when the caller gave
+// none (krige_set_sim without them, or none before solve)
+void engine_sim_defaults(Engine& e, bool path, bool sample);
 // FP64 re-solve of the last solve's neighbour sets without any device
 // allocation (workspace in a fixed static array); value (nobs) replaces the
 // observation values of variable ivar first when it is not null.

@@ -106,6 +106,31 @@ void launch_search_kdtree(const KkSearch& S, const int* list, const int* count, 
                           const double* const* ox, int* nbr, int* nnear, int* status, void* heaps,
                           int heap_stride, int nthreads, cudaStream_t st);
 size_t kd_heap_entry_bytes();
+// Neighbour lists of a sequential simulation's targets (in visiting order)
+// over the nobs observations followed by the targets; heaps: nthreads x
+// heap_stride (>= nmax + 2) entries of kd_heap_entry_bytes().
+void launch_search_sgsim(const KkSearch& S, int ntarget, int nobs, const double* const* tx, const double* const* ox,
+                         int* nbr, int* nnear, void* heaps, int heap_stride, int nthreads, cudaStream_t st);
+// One dependency level of a sequential simulation: for every target p of
+// list[0, count) (visiting positions) and realisation s, the kriged value
+// from the stored weights over the observations and the simulated targets,
+// plus sqrt(max(var, 0)) * sample[p * nsim + s]; written to sim[s * nb + p]
+// and to out[(path[p] - 1) * nsim + s].
+struct SimParams {
+  const int* nbr;       // (nb, mmax) neighbour lists, row order of the weights
+  const int* nnear;     // (nb)
+  const double* w;      // (nb, wstride) kriging weights
+  const double* var;    // (nb) conditional variance
+  const double* z;      // (nobs) observation values
+  const double* sample; // (nb, nsim)
+  const int* path;      // (nb) 1-based target of each visiting position
+  double* sim;          // (nsim, nb) simulated values by visiting position
+  double* out;          // (nb targets, nsim)
+  int nb, nobs, nsim, mmax, wstride;
+  int sk;               // simple kriging: the mean term on the observation weights
+  double sk_mean, lo, hi;
+};
+void launch_sgsim_level(const SimParams& S, const int* list, int count, int nsm, cudaStream_t st);
 
 void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
 // Estimates of every target from the weight store (P.wout, P.nbr, P.nnear)

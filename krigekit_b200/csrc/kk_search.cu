@@ -1023,8 +1023,10 @@ __device__ void kd_heapsort(KdHeapEntry* a, int n) {
 }
 
 // kdtree2_n_nearest (kdtree2_maxidx.f90:1043-1085) with search and
-// process_terminal_node (1383-1612) unrolled onto an explicit stack.
-__device__ void kd_n_nearest(const KkTree& T, const double* qv, int nn, KdHeapEntry* heap) {
+// process_terminal_node (1383-1612) unrolled onto an explicit stack; points
+// with index >= maxn are skipped before their distance is taken (the
+// _maxidx variants, kdtree2_maxidx.f90:1928-2110).
+__device__ void kd_n_nearest(const KkTree& T, const double* qv, int nn, KdHeapEntry* heap, int maxn = 0x7fffffff) {
   struct Frame { int node; int phase; double dis; };
   Frame stack[192];
   int sp = 0;
@@ -1039,6 +1041,7 @@ __device__ void kd_n_nearest(const KkTree& T, const double* qv, int nn, KdHeapEn
       if (!(left >= 0 && right >= 0)) {
         double bs = ballsize;
         for (int i = l; i <= u; ++i) {
+          if (T.ind[i] >= maxn) continue;
           double sd = 0.0;
           bool skip = false;
           for (int k = 0; k < T.D; ++k) {
@@ -1152,6 +1155,81 @@ __global__ void k_search_kdtree(KkSearch S, const int* __restrict__ list, const 
   }
 }
 
+// Neighbours of the targets of a sequential simulation (search_neighbors,
+// simulation branch, kriging.F90:524-612), one thread per target: the
+// observation set here is the nobs observations followed by the targets in
+// visiting order, and target p may use the observations and the targets
+// visited before it (indices < nobs + p).  The nmax nearest of those
+// (kdtree2_n_nearest_maxidx, heap order), or all of them when nmax does not
+// cut; the simulated members are cut by maxdist and dropped when co-located
+// with an observation neighbour (relative tolerance 1e-6).  The list is the
+// observation members ascending, then the simulated members in heap order:
+// the reference's matrix order.  heaps holds nmax + 2 entries per thread.
+__global__ void k_search_sgsim(KkSearch S, int ntarget, int nobs, const double* __restrict__ t0,
+                               const double* __restrict__ t1, const double* __restrict__ t2,
+                               const double* __restrict__ ox0, const double* __restrict__ ox1,
+                               const double* __restrict__ ox2, int* __restrict__ nbr, int* __restrict__ nnear,
+                               KdHeapEntry* __restrict__ heaps, int heap_stride) {
+  const double* ts[3] = {t0, t1, t2};
+  const double* os[3] = {ox0, ox1, ox2};
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  KdHeapEntry* h = heaps + (size_t)gt * heap_stride;
+  for (int p = gt; p < ntarget; p += gridDim.x * blockDim.x) {
+    double x[3] = {0.0, 0.0, 0.0}, q[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < S.ndim; ++d) x[d] = ts[d][p];
+    if (S.aniso) rotate_pt(S.rotmat, S.ndim, x, q);
+    else for (int d = 0; d < S.ndim; ++d) q[d] = x[d];
+    int* out = nbr + (size_t)p * S.mmax;
+    const int lim = nobs + p;
+    int no = 0, nb = 0;
+    // members: observations go to out[0 ..), simulated ones to h[1 ..) as (dis, index)
+    if (S.nmax < lim) {
+      kd_n_nearest(S.tree, q, S.nmax, h, lim);
+      for (int i = 1; i <= S.nmax; ++i) {
+        const int idx = h[i].idx;
+        if (idx < nobs) out[no++] = idx;
+        else h[1 + nb++] = h[i];
+      }
+    } else {
+      for (int i = 0; i < nobs; ++i) out[no++] = i;
+      for (int j = 0; j < p; ++j) {  // rotated_dists of the raw centres (rotation.f90:193-218)
+        double diff[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < S.ndim; ++d) diff[d] = dsub(os[d][nobs + j], q[d]);
+        rotate_pt(S.rotmat, S.ndim, diff, r);
+        double s2 = 0.0;
+        for (int d = 0; d < S.ndim; ++d) s2 = dadd(s2, dmul(r[d], r[d]));
+        h[1 + nb].dis = s2;
+        h[1 + nb].idx = nobs + j;
+        ++nb;
+      }
+    }
+    // maxdist on the simulated members (filter_by_maxlag, kriging_base.F90:2491-2505),
+    // then the ones co-located with an observation member (kriging.F90:584-609)
+    int keep = 0;
+    for (int i = 1; i <= nb; ++i) {
+      if (!(h[i].dis <= S.maxd2)) continue;
+      const int idx = h[i].idx;
+      bool dup = false;
+      for (int o = 0; o < no && !dup; ++o) {
+        dup = true;
+        for (int d = 0; d < S.ndim; ++d) {
+          const double xo = os[d][out[o]];
+          if (fabs(os[d][idx] - xo) > 1.0e-6 * (1.0 + fabs(xo))) { dup = false; break; }
+        }
+      }
+      if (!dup) h[1 + keep++] = h[i];
+    }
+    // isort of the observation members (kriging_base.F90:3510-3524)
+    for (int i = 1; i < no; ++i) {
+      int tmp = out[i], j = i - 1;
+      while (j >= 0 && out[j] > tmp) { out[j + 1] = out[j]; --j; }
+      out[j + 1] = tmp;
+    }
+    for (int i = 0; i < keep; ++i) out[no + i] = h[1 + i].idx;
+    nnear[p] = no + keep;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -1205,5 +1283,12 @@ void launch_search_kdtree(const KkSearch& S, const int* list, const int* count, 
 }
 
 size_t kd_heap_entry_bytes() { return sizeof(KdHeapEntry); }
+
+void launch_search_sgsim(const KkSearch& S, int ntarget, int nobs, const double* const* tx, const double* const* ox,
+                         int* nbr, int* nnear, void* heaps, int heap_stride, int nthreads, cudaStream_t st) {
+  const int blocks = (nthreads + 63) / 64;
+  k_search_sgsim<<<blocks, 64, 0, st>>>(S, ntarget, nobs, tx[0], tx[1], tx[2], ox[0], ox[1], ox[2], nbr, nnear,
+                                       static_cast<KdHeapEntry*>(heaps), heap_stride);
+}
 
 }  // namespace kk

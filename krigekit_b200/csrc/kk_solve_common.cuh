@@ -172,6 +172,31 @@ static __device__ __noinline__ void finish_outputs(const SolveParams& P, int t, 
   }
 }
 
+// finish_outputs for one variable with one unbiasedness row and z as the
+// only functional column (ordinary kriging, columns F | k | z): the same
+// arithmetic in the same order, in registers, with no call frame.
+__device__ __forceinline__ void finish_ok(const SolveParams& P, int t, const double* G, int* fail) {
+  const double s00 = G[0];
+  if (!(s00 > 0.0)) {
+    *fail = 1;
+    return;
+  }
+  const double ajj = sqrt(s00);
+  double lam = G[1] - g_entry(P, 0, 0, t);
+  lam = lam / ajj;
+  lam = lam / ajj;
+  double avg = G[7];
+  avg -= G[6] * lam;
+  if (avg < P.bounds[0]) avg = P.bounds[0];
+  if (avg > P.bounds[1]) avg = P.bounds[1];
+  P.est[t] = avg;
+  double d = G[4];
+  d -= lam * G[1];
+  d += lam * g_entry(P, 0, 0, t);
+  const double v = base_cov(P, t, 0, 0) - d;
+  P.var[t] = v < 0.0 ? 0.0 : v;
+}
+
 // Covariance of one neighbour row (coordinates xr, variable vr) with the
 // target for target variable iv, averaged over block nodes (assemble_rhs,
 // kriging.F90:889-910); defined after the fast covariance paths.

@@ -564,7 +564,10 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
     __syncwarp();
     int f = 0;
     if (lane == 0) {
-      finish_outputs(P, t, s.G, C, s.zmean, &f, WT ? s.lam : nullptr);
+      // the FP64 forms finish ordinary kriging in registers; the refinement
+      // form keeps the out-of-line routine (its 128-register budget is full)
+      if (!REFINE && !WT && C == 3 && P.pa == 1 && q == 1) finish_ok(P, t, s.G, &f);
+      else finish_outputs(P, t, s.G, C, s.zmean, &f, WT ? s.lam : nullptr);
       if (f) {
         P.status[t] |= KK_ST_LDLT;
         const int p = atomicAdd(&P.counters[KK_CNT_FB], 1);

@@ -290,6 +290,46 @@ class Kriging:
                   float(dip), float(plunge), int(bool(sector_search)))
 
     # -------------------------------------------------------------------- solve
+    def set_sim(self, randpath: Optional[np.ndarray] = None, sample: Optional[np.ndarray] = None):
+        """Sequential Gaussian simulation: visiting order and N(0, 1) draws
+        (kriging.py:1134-1203).  randpath is a 1-based permutation of the
+        targets; sample is (nblocks,), (nblocks, nsim) or (nblocks, nvar,
+        nsim), row p taken by the p-th visited target.  Either may be None:
+        the library then draws them from the constructor's seed (its own
+        generator, not the reference's)."""
+        if self.nsim <= 0:
+            raise AssertionError("nsim must be > 0 when setting SGSIM parameters.")
+        nb = self._nb()
+        rp_ptr = ctypes.c_void_p(0)
+        s_ptr = ctypes.c_void_p(0)
+        nsim_c = nvar_c = 0
+        nblocks = nb
+        keep = []
+        if randpath is not None:
+            rp = np.ascontiguousarray(np.asarray(randpath, dtype=np.int32).ravel())
+            if rp.size != nb:
+                raise ValueError(f"randpath length ({rp.size}) must match nblocks ({nb})")
+            if not np.array_equal(np.sort(rp), np.arange(1, nb + 1, dtype=np.int32)):
+                raise ValueError("randpath must be a 1-based permutation of 1..nblocks")
+            rp_ptr = ctypes.c_void_p(rp.ctypes.data)
+            keep.append(rp)
+        if sample is not None:
+            sa = np.asarray(sample, dtype=np.float64)
+            if sa.ndim == 1:
+                sa = sa[:, np.newaxis, np.newaxis]
+            elif sa.ndim == 2:
+                sa = sa[:, np.newaxis, :]
+            elif sa.ndim != 3:
+                raise ValueError(f"sample must be 2-D (nblocks, nsim) or 3-D (nblocks, nvar, nsim), got shape {sa.shape}")
+            sf = _drift_to_fortran(sa)  # (nsim, nvar, nblocks) column-major
+            nsim_c, nvar_c, n_s = sf.shape
+            if nsim_c != self.nsim or nvar_c != self.nvar or n_s != nb:
+                raise ValueError(f"sample shape ({nsim_c}, {nvar_c}, {n_s}) must be ({self.nsim}, {self.nvar}, {nb})")
+            s_ptr = ctypes.c_void_p(sf.ctypes.data)
+            keep.append(sf)
+        _lib.call("krige_set_sim", self._h(), nblocks, rp_ptr, nsim_c, nvar_c, s_ptr)
+        self._set_sim = True
+
     def solve(self, nthread: int = 0, ncache: Optional[int] = None):
         """Run the kriging solve on the GPU (kriging.py:1321-1344)."""
         _lib.call("krige_solve", self._h(), int(nthread), -1 if ncache is None else int(ncache))
@@ -357,7 +397,7 @@ class Kriging:
 
     def get_results(self, copy: bool = False, squeeze: bool = True):
         """(estimate, variance) as in kriging.py:1382-1440."""
-        nb, nv, ns = self._nb(), self.nvar, 1
+        nb, nv, ns = self._nb(), self.nvar, max(1, self.nsim)
         estimate = _fempty((nb, nv, ns))
         variance = _fempty((nb, nv, nv))
         _lib.call("krige_get_estimate_all", self._h(), nb, nv, ns, _dptr(estimate))
@@ -511,6 +551,27 @@ class Kriging:
 
     def __repr__(self):
         return f"Kriging(ndim={self.ndim}, nvar={self.nvar}, precision={self.precision!r}, device={self.device})"
+
+
+def sequential_gaussian_simulation(obs_coord, obs_value, grid_coord, vgm_spec, nsim: int, nmax=None,
+                                   randpath=None, sample=None, seed=None, rangescale=None, localnugget=None,
+                                   nthread: int = 0, ncache=None) -> np.ndarray:
+    """Sequential Gaussian simulation of one variable (kriging.py:2144-2205):
+    (ngrid,) for one realisation, (ngrid, nsim) for several, in target order."""
+    obs_coord = np.asarray(obs_coord, dtype=np.float64)
+    ndim = obs_coord.shape[1]
+    if nmax is None:
+        nmax = len(obs_coord) + len(grid_coord)
+    k = Kriging(ndim=ndim, nvar=1, nsim=nsim, seed=seed)
+    k.set_obs(ivar=1, coord=obs_coord, value=obs_value, nmax=nmax)
+    k.set_grid(coord=grid_coord, rangescale=rangescale, localnugget=localnugget)
+    for spec in ([vgm_spec] if isinstance(vgm_spec, dict) else list(vgm_spec)):
+        k.set_vgm(ivar=1, jvar=1, **spec)
+    k.set_sim(randpath, sample)
+    k.set_search(ivar=1)
+    k.solve(nthread=nthread, ncache=ncache)
+    sims, _ = k.get_results()
+    return sims
 
 
 def ordinary_kriging(obs_coord, obs_value, grid_coord, vgm_spec, nmax=None, maxdist=None, search_anis1=1.0,

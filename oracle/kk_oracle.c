@@ -13,6 +13,7 @@
 #include "kk_oracle.h"
 
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -618,6 +619,7 @@ typedef struct {
   int nn, nfound;
   double ballsize;
   kd_res *heap;   /* 1-based, size nn+1 */
+  int maxn;       /* only points with 0-based index < maxn (the _maxidx variants) */
 } kd_search_rec;
 
 /* pq_insert, kdtree2_maxidx.f90:307-349 */
@@ -666,6 +668,7 @@ static void kd_terminal(kd_search_rec *sr, const kd_node *nd) {
   double ballsize = sr->ballsize;
   const int D = t->dimen;
   for (int i = nd->l; i <= nd->u; ++i) {
+    if (t->ind[i] >= sr->maxn) continue; /* process_terminal_node_maxidx, kdtree2_maxidx.f90:2081 */
     double sd = 0.0;
     int skip = 0;
     for (int k = 0; k < D; ++k) {
@@ -748,8 +751,10 @@ static void kd_heapsort(kd_res *a, int n) {
   }
 }
 
-/* kdtree2_n_nearest, kdtree2_maxidx.f90:1043-1085; heap is 1-based [nn+1] */
-static void kd_n_nearest(const kd_tree *t, const double *qv, int nn, int sort, kd_res *heap) {
+/* kdtree2_n_nearest, kdtree2_maxidx.f90:1043-1085, and
+ * kdtree2_n_nearest_maxidx, :1928-1964 (maxn = max_idx as a 0-based bound);
+ * heap is 1-based [nn+1] */
+static void kd_n_nearest_max(const kd_tree *t, const double *qv, int nn, int sort, kd_res *heap, int maxn) {
   kd_search_rec sr;
   sr.t = t;
   sr.qv = qv;
@@ -757,8 +762,13 @@ static void kd_n_nearest(const kd_tree *t, const double *qv, int nn, int sort, k
   sr.nfound = 0;
   sr.ballsize = DBL_MAX;
   sr.heap = heap;
+  sr.maxn = maxn;
   kd_search(&sr, t->root);
   if (sort) kd_heapsort(heap, nn);
+}
+
+static void kd_n_nearest(const kd_tree *t, const double *qv, int nn, int sort, kd_res *heap) {
+  kd_n_nearest_max(t, qv, nn, sort, heap, INT_MAX);
 }
 
 int orc_kdtree_nn(const double *data, int dim, int n, const double *qv, int nn,
@@ -1686,6 +1696,238 @@ done:
       else { model_free(&c->smdl[a][b].cs); model_free(&c->smdl[a][b].ct); }
     }
   free(c->gstart);
+  free(c);
+  return R->err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* sequential Gaussian simulation of one variable                           */
+/* ------------------------------------------------------------------------ */
+/* set_sim_base (kriging_base.F90:1226-1320): the targets are visited in the
+ * order of path (1-based), the simulated targets join the observations as a
+ * second neighbour group (obs%coord extended by the block centres in path
+ * order).  Per visited target (search_neighbors, kriging.F90:524-612):
+ * the nmax nearest among the observations and the targets visited before it
+ * (kdtree2_n_nearest_maxidx), or all of them when nmax does not cut; the
+ * simulated group keeps the heap order, is cut by maxdist, and loses members
+ * co-located with an observation neighbour.  The system carries the
+ * observation group (sorted, with its measurement variance) and the
+ * simulated group (no measurement variance) (assemble_lhs / assemble_rhs,
+ * kriging.F90:740-939); the draw adds the simulated group's values and the
+ * square root of the conditional variance times the sample
+ * (estimate_block_base + sim_draw_base, kriging_base.F90:3473-3495, 2320-2327);
+ * results return to target order (reorder_sgsim_base, :2268-2282). */
+int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int nsim, orc_sim_result *R) {
+  R->err = 0;
+  R->errmsg[0] = 0;
+  if (P->nvar != 1 || P->st || P->nblockpnt || P->sector[0] || P->ndrift > 0 || P->cross_validation) {
+    R->err = 1;
+    snprintf(R->errmsg, 256, "sgsim: one variable, point targets, no sectors, drift or cross-validation");
+    return 1;
+  }
+  const int nb = P->nblock, nobs = P->nobs[0], ndim = P->ndim, nlag = ndim;
+  const int ntot = nobs + nb;
+  int nmax = P->nmax[0];
+  if (nmax <= 0 || nmax > ntot) nmax = ntot;
+  orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
+  c->p = P;
+  c->nvar = 1;
+  c->ndim = ndim;
+  c->nlag = nlag;
+  c->naug = P->unbias;
+  c->pa = c->naug;
+  const int pa = c->pa;
+  if (P->nstruct[0][0] == 0) {
+    R->err = 1;
+    snprintf(R->errmsg, 256, "variogram not set for ivar=1, jvar=1");
+    free(c);
+    return 1;
+  }
+  model_init(&c->mdl[0][0], ndim, P->vgm[0][0], P->nstruct[0][0]);
+  model_build_table(&c->mdl[0][0]);
+  double a1 = P->s_anis1[0] != 0.0 ? P->s_anis1[0] : 1.0;
+  double a2 = P->s_anis2[0] != 0.0 ? P->s_anis2[0] : 1.0;
+  const int aniso = (fabs(a1 - 1.0) > ORC_EPSLON || fabs(a2 - 1.0) > ORC_EPSLON) && P->anisotropic_search;
+  double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (aniso) orc_calc_rotmat(P->s_az[0], P->s_dip[0], P->s_plunge[0], a1, a2, rot);
+  const double maxd2 = P->maxdist[0] * P->maxdist[0];
+
+  /* observations, then the targets in visiting order */
+  double *xc = (double *)malloc(sizeof(double) * (size_t)ntot * nlag);
+  double *sc = (double *)malloc(sizeof(double) * (size_t)ntot * nlag);
+  for (int i = 0; i < nobs; ++i)
+    for (int d = 0; d < nlag; ++d) xc[(size_t)i * nlag + d] = P->obs_coord[0][(size_t)i * nlag + d];
+  for (int p = 0; p < nb; ++p)
+    for (int d = 0; d < nlag; ++d)
+      xc[(size_t)(nobs + p) * nlag + d] = P->block_coord[(size_t)(path[p] - 1) * nlag + d];
+  for (int i = 0; i < ntot; ++i) {
+    if (aniso) rotate_pt(rot, ndim, xc + (size_t)i * nlag, sc + (size_t)i * nlag);
+    else for (int d = 0; d < ndim; ++d) sc[(size_t)i * nlag + d] = xc[(size_t)i * nlag + d];
+  }
+  kd_tree tree;
+  kd_create(&tree, sc, nlag, ntot);
+  double *vals = (double *)malloc(sizeof(double) * (size_t)nsim * nb);  /* [isim][path position] */
+  kd_res *h = (kd_res *)malloc(sizeof(kd_res) * ((size_t)nmax + 1));
+  int *io = (int *)malloc(sizeof(int) * ((size_t)ntot + 1));
+  int *ib_ = (int *)malloc(sizeof(int) * ((size_t)ntot + 1));
+  double *db = (double *)malloc(sizeof(double) * ((size_t)ntot + 1));
+  const int mm = nmax + pa;
+  double *A = (double *)malloc(sizeof(double) * (size_t)mm * mm);
+  double *B = (double *)malloc(sizeof(double) * mm);
+  double *X = (double *)malloc(sizeof(double) * mm);
+  double *work = (double *)malloc(sizeof(double) * ((size_t)mm * 2 + (size_t)mm * mm));
+  orc_fac f;
+  memset(&f, 0, sizeof f);
+  f.L = (double *)malloc(sizeof(double) * (size_t)mm * mm);
+  f.Y = (double *)malloc(sizeof(double) * (size_t)mm * (pa > 0 ? pa : 1));
+  f.S = (double *)malloc(sizeof(double) * (pa > 0 ? pa * pa : 1));
+  f.Afac = (double *)malloc(sizeof(double) * (size_t)mm * mm);
+  f.ipiv = (int *)malloc(sizeof(int) * mm);
+  const double cov0 = c->mdl[0][0].cov0;
+
+  for (int p = 0; p < nb && !R->err; ++p) {
+    const int node = path[p] - 1;
+    const double *xloc = P->block_coord + (size_t)node * nlag;
+    const double rs = P->rangescale ? P->rangescale[node] : 1.0;
+    const double ln = P->localnugget ? P->localnugget[node] : 0.0;
+    double newloc[3];
+    if (aniso) rotate_pt(rot, ndim, xloc, newloc);
+    else for (int d = 0; d < ndim; ++d) newloc[d] = xloc[d];
+    int no = 0, nbk = 0;
+    const int lim = nobs + p;
+    if (nmax < lim) {
+      kd_n_nearest_max(&tree, newloc, nmax, 0, h, lim);
+      for (int i = 1; i <= nmax; ++i) {
+        if (h[i].idx < nobs) io[no++] = h[i].idx;
+        else { ib_[nbk] = h[i].idx - nobs; db[nbk] = h[i].dis; ++nbk; }
+      }
+    } else {
+      for (int i = 0; i < nobs; ++i) io[no++] = i;
+      for (int q = 0; q < p; ++q) {  /* rotated_dists of the raw block centres (rotation.f90:193-218) */
+        double diff[3], r[3];
+        for (int d = 0; d < ndim; ++d) diff[d] = xc[(size_t)(nobs + q) * nlag + d] - newloc[d];
+        rotate_pt(rot, ndim, diff, r);
+        double s2 = 0.0;
+        for (int d = 0; d < ndim; ++d) s2 = s2 + r[d] * r[d];
+        ib_[nbk] = q;
+        db[nbk] = s2;
+        ++nbk;
+      }
+    }
+    /* filter_by_maxlag on the simulated group (kriging_base.F90:2491-2505) */
+    int k2 = 0;
+    for (int i = 0; i < nbk; ++i)
+      if (db[i] <= maxd2) { ib_[k2] = ib_[i]; db[k2] = db[i]; ++k2; }
+    nbk = k2;
+    /* simulated targets co-located with an observation neighbour, kriging.F90:584-609 */
+    if (no > 0 && nbk > 0) {
+      k2 = 0;
+      for (int jb = 0; jb < nbk; ++jb) {
+        int dup = 0;
+        for (int oo = 0; oo < no; ++oo) {
+          dup = 1;
+          for (int d = 0; d < ndim; ++d) {
+            const double xo = xc[(size_t)io[oo] * nlag + d];
+            if (fabs(xc[(size_t)(nobs + ib_[jb]) * nlag + d] - xo) > 1.0e-6 * (1.0 + fabs(xo))) { dup = 0; break; }
+          }
+          if (dup) break;
+        }
+        if (!dup) { ib_[k2] = ib_[jb]; db[k2] = db[jb]; ++k2; }
+      }
+      nbk = k2;
+    }
+    isort(io, no);
+    if (R->nnear) { R->nnear[(size_t)node * 2] = no; R->nnear[(size_t)node * 2 + 1] = nbk; }
+    if (R->inear) {
+      for (int i = 0; i < no; ++i) R->inear[(size_t)node * R->mmax + i] = io[i];
+      for (int i = 0; i < nbk; ++i) R->inear[(size_t)node * R->mmax + no + i] = nobs + ib_[i];
+    }
+    const int npp = no + nbk, m = npp + pa;
+    double var = NAN;
+    double *vrow = R->value + (size_t)node * nsim;
+    if (npp == 0) {
+      for (int is = 0; is < nsim; ++is) { vrow[is] = NAN; vals[(size_t)is * nb + p] = NAN; }
+      R->variance[node] = NAN;
+      continue;
+    }
+    /* row coordinates: observation group, then the simulated group */
+#define SG_X(k) ((k) < no ? xc + (size_t)io[(k)] * nlag : xc + (size_t)(nobs + ib_[(k) - no]) * nlag)
+    for (size_t q = 0; q < (size_t)m * m; ++q) A[q] = 0.0;
+    for (int i = 0; i < npp; ++i) {
+      const double ov = (i < no && P->obs_var[0]) ? P->obs_var[0][io[i]] : 0.0;
+      A[i + (size_t)i * m] = cov0 + ov + ln;
+      for (int j = i + 1; j < npp; ++j) {
+        double lag[4];
+        lag_of(c, SG_X(i), SG_X(j), rs, lag);
+        A[j + (size_t)i * m] = pair_cov(c, 0, 0, lag);
+      }
+      for (int r = 0; r < pa; ++r) A[(npp + r) + (size_t)i * m] = 1.0;
+    }
+    for (int ir = 0; ir < npp; ++ir)
+      for (int ic = ir + 1; ic < m; ++ic) A[ir + (size_t)ic * m] = A[ic + (size_t)ir * m];
+    for (int k = 0; k < npp; ++k) {
+      double lag[4];
+      lag_of(c, SG_X(k), xloc, rs, lag);
+      B[k] = pair_cov(c, 0, 0, lag);
+    }
+    for (int r = 0; r < pa; ++r) B[npp + r] = 1.0;
+#undef SG_X
+    int info = chol_setup(npp, pa, A, m, &f);
+    if (info == 0) {
+      chol_solve(npp, pa, 1, &f, B, X, work);
+    } else {
+      for (size_t q = 0; q < (size_t)m * m; ++q) f.Afac[q] = A[q];
+      info = sytf2_u(m, f.Afac, m, f.ipiv);
+      if (info != 0) {
+        double dscale = 0.0;
+        for (int ii = 0; ii < npp; ++ii) dscale = dscale + A[ii + (size_t)ii * m];
+        if (dscale > 0.0) {
+          dscale = 1.0e-6 * (dscale / (double)npp);
+          for (int ii = 0; ii < npp; ++ii) A[ii + (size_t)ii * m] = A[ii + (size_t)ii * m] + dscale;
+          for (size_t q = 0; q < (size_t)m * m; ++q) f.Afac[q] = A[q];
+          info = sytf2_u(m, f.Afac, m, f.ipiv);
+        }
+      }
+      if (info == 0) ldl_solve(m, 1, &f, B, X, work);
+    }
+    if (info != 0) {
+      if (!P->neglect_error) {
+        R->err = 1;
+        snprintf(R->errmsg, 256, "Singular matrix at block %d", node + 1);
+        break;
+      }
+      for (int is = 0; is < nsim; ++is) { vrow[is] = NAN; vals[(size_t)is * nb + p] = NAN; }
+      R->variance[node] = NAN;
+      continue;
+    }
+    double s = 0.0;
+    for (int k = 0; k < m; ++k) s = s + X[k] * B[k];
+    var = cov0 - s;
+    if (!(var >= 0.0) && !isnan(var)) var = 0.0;
+    R->variance[node] = var;
+    double avg = 0.0, tw = 0.0;
+    for (int k = 0; k < no; ++k) {
+      tw = tw + X[k];
+      avg = avg + P->obs_value[0][io[k]] * X[k];
+    }
+    if (P->unbias == 0 && P->sk_mean[0] != 0.0) avg = avg + (1.0 - tw) * P->sk_mean[0];
+    const double L = sqrt(var > 0.0 ? var : 0.0);
+    for (int is = 0; is < nsim; ++is) {
+      double v = avg, dp = 0.0;
+      for (int k = 0; k < nbk; ++k) dp = dp + vals[(size_t)is * nb + ib_[k]] * X[no + k];
+      v = v + dp;
+      v = v + L * sample[(size_t)p * nsim + is];
+      if (v < P->bounds[0]) v = P->bounds[0];
+      if (v > P->bounds[1]) v = P->bounds[1];
+      vals[(size_t)is * nb + p] = v;
+      vrow[is] = v;
+    }
+  }
+  free(f.L); free(f.Y); free(f.S); free(f.Afac); free(f.ipiv);
+  free(A); free(B); free(X); free(work); free(h); free(io); free(ib_); free(db); free(vals);
+  kd_free(&tree);
+  free(xc); free(sc);
+  model_free(&c->mdl[0][0]);
   free(c);
   return R->err;
 }

@@ -100,6 +100,22 @@ typedef struct {
 
 int orc_solve(const orc_problem *prob, orc_result *res);
 
+/* Sequential Gaussian simulation of one variable over the point targets of
+ * prob (set_sim_base and the simulation branches of the reference engine):
+ * path holds the 1-based visiting order, sample the N(0, 1) draws as
+ * sample[p * nsim + isim] for the p-th visited target. */
+typedef struct {
+  double *value;        /* (nsim, nblock): value[ib * nsim + isim], target order */
+  double *variance;     /* (nblock) conditional variance of each target          */
+  int *nnear;           /* (2, nblock): observation and simulated neighbours, or NULL */
+  int *inear;           /* (mmax, nblock): 0-based; observations < nobs, then nobs + visit position; or NULL */
+  int mmax;
+  int err;
+  char errmsg[256];
+} orc_sim_result;
+
+int orc_sgsim(const orc_problem *prob, const int *path, const double *sample, int nsim, orc_sim_result *res);
+
 /* Building blocks exported for unit tests. */
 void orc_calc_rotmat(double ang1, double ang2, double ang3, double anis1,
                      double anis2, double *out /* column-major 3x3 */);

@@ -89,6 +89,11 @@ class _Result(ctypes.Structure):
                 ("errmsg", ctypes.c_char * 256)]
 
 
+class _SimResult(ctypes.Structure):
+    _fields_ = [("value", _PD), ("variance", _PD), ("nnear", _PI), ("inear", _PI), ("mmax", _I),
+                ("err", _I), ("errmsg", ctypes.c_char * 256)]
+
+
 _lib = None
 
 
@@ -105,6 +110,8 @@ def lib():
         _lib.orc_kdtree_nn.argtypes = [_PD, _I, _I, _PD, _I, _I, _PD, _PI]
         _lib.orc_sysv.argtypes = [_I, _PD, _I, _PD]
         _lib.orc_sysv.restype = _I
+        _lib.orc_sgsim.argtypes = [ctypes.POINTER(_Problem), _PI, _PD, _I, ctypes.POINTER(_SimResult)]
+        _lib.orc_sgsim.restype = _I
     return _lib
 
 
@@ -120,8 +127,9 @@ class OracleKriging:
     def __init__(self, ndim: int = 2, nvar: int = 1, ndrift: int = 0, unbias: int = 1,
                  nsim: int = 0, anisotropic_search: bool = False, neglect_error: bool = True,
                  std_ck: bool = False, bounds: Optional[tuple] = None, nmin: int = 0, **_ignored):
-        if nsim:
-            raise ValueError("the oracle covers kriging only (nsim == 0)")
+        self.nsim = int(nsim)
+        self.sim_path = None
+        self.sim_sample = None
         self.ndim, self.nvar, self.ndrift, self.unbias = ndim, nvar, ndrift, unbias
         self.nlag = ndim
         self.anisotropic_search = anisotropic_search
@@ -322,8 +330,44 @@ class OracleKriging:
     def _fill_st(self, P):
         P.st = 0
 
+    def set_sim(self, randpath, sample):
+        """SGSIM visiting order (1-based, nblock) and N(0, 1) draws: (nblock,),
+        (nblock, nsim) or (nblock, 1, nsim) like the reference's set_sim
+        (kriging.py:1134-1203); the p-th visited target takes row p."""
+        self.sim_path = np.ascontiguousarray(np.asarray(randpath, dtype=np.int32).ravel())
+        smp = np.asarray(sample, dtype=np.float64)
+        smp = smp.reshape(smp.shape[0], -1)
+        if smp.shape[1] != self.nsim:
+            raise ValueError("sample needs nsim columns")
+        self.sim_sample = np.ascontiguousarray(smp)
+        return self
+
+    def _solve_sim(self):
+        P, keep = self._problem(nthread=1, ncache=0)
+        nb = P.nblock
+        nmax = int(self.obs[0]["nmax"])
+        mm = min(max(nmax, 1), self.obs[0]["coord"].shape[0] + nb)
+        self.value = np.full((nb, self.nsim), np.nan)
+        self.variance = np.full(nb, np.nan)
+        self.sim_nnear = np.zeros((nb, 2), dtype=np.int32)
+        self.sim_inear = np.zeros((nb, mm), dtype=np.int32)
+        R = _SimResult()
+        R.value = _dp(self.value)
+        R.variance = _dp(self.variance)
+        R.nnear = self.sim_nnear.ctypes.data_as(_PI)
+        R.inear = self.sim_inear.ctypes.data_as(_PI)
+        R.mmax = mm
+        ierr = lib().orc_sgsim(ctypes.byref(P), self.sim_path.ctypes.data_as(_PI), _dp(self.sim_sample),
+                               self.nsim, ctypes.byref(R))
+        if ierr:
+            raise RuntimeError(R.errmsg.decode())
+        self._keep = keep
+        return self
+
     def solve(self, nthread: int = 0, ncache: Optional[int] = 64, keep_neighbours: bool = True,
               keep_weights: bool = False):
+        if self.nsim > 0:
+            return self._solve_sim()
         P, keep = self._problem(nthread=nthread, ncache=64 if ncache is None else ncache)
         nb, nv = P.nblock, self.nvar
         mmax = 1
@@ -363,6 +407,8 @@ class OracleKriging:
     def get_results(self, squeeze: bool = True):
         est = self.value.copy()
         var = self.variance.copy()
+        if self.nsim > 0:  # (nblock, nsim) realisations, (nblock,) conditional variance
+            return (est[:, 0] if squeeze and self.nsim == 1 else est), var
         if squeeze and self.nvar == 1:
             return est[:, 0], var[:, 0, 0]
         return est, var

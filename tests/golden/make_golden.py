@@ -25,8 +25,10 @@ def main(ref_root: str) -> None:
     # grid2d.csv: 4800 targets with the reference ordinary-kriging estimate/variance
     pd.read_csv(os.path.join(td, "grid2d.csv"))[["x", "y", "estimate", "variance"]].to_csv(
         os.path.join(HERE, "grid2d.csv"), index=False)
+    # path4800.csv / sample4800.csv: the SGSIM visiting order and N(0, 1) draws of
+    # the reference's deterministic simulation test (tests/test_sgsim.py)
     for name in ("obs_simple.csv", "grid_simple.csv", "head2d.csv", "walker.csv",
-                 "gridblockpnt2d.csv"):
+                 "gridblockpnt2d.csv", "path4800.csv", "sample4800.csv"):
         pd.read_csv(os.path.join(td, name)).to_csv(os.path.join(HERE, name), index=False)
     blk = pd.read_csv(os.path.join(td, "gridblock2d.csv"))
     blk.columns = [c.strip().lstrip("#").strip() for c in blk.columns]
