@@ -205,3 +205,70 @@ def test_kdtree_exact_knn():
     d2 = ((data - q) ** 2).sum(1)
     assert set(idx - 1) == set(np.argsort(d2)[:25])
     assert np.all(np.diff(dis) >= 0)
+
+
+# --------------------------------------------------------------------------
+# sequential Gaussian simulation (orc_sgsim): the reference's behaviours
+# --------------------------------------------------------------------------
+_VGM_PC2D = dict(vtype="sph", nugget=0.0, sill=0.12, a_major=5000.0)
+
+
+def _sgsim_pc2d(path, sample, nsim=1, nmax=20):
+    pc = pd.read_csv(golden("pc2d.csv"))
+    gr = pd.read_csv(golden("grid2d.csv"))
+    o = OracleKriging(ndim=2, nvar=1, nsim=nsim)
+    o.set_obs(1, pc[["x", "y"]].values, pc["pc"].values, nmax=nmax)
+    o.set_vgm(1, 1, **_VGM_PC2D)
+    o.set_grid(gr[["x", "y"]].values)
+    o.set_search(1)
+    o.set_sim(path, sample)
+    return o.solve(), pc, gr
+
+
+def test_sgsim_reference_regression_case():
+    """tests/test_sgsim.py::test_class_interface_with_precomputed_path_sample:
+    the stored path and draws give finite realisations within [-5, 5]."""
+    path = pd.read_csv(golden("path4800.csv"))["randpath"].values
+    sample = pd.read_csv(golden("sample4800.csv"))["sample"].values
+    o, _, gr = _sgsim_pc2d(path, sample)
+    sims, var = o.get_results()
+    assert sims.shape == (len(gr),) and np.isfinite(sims).all()
+    assert sims.min() >= -5.0 and sims.max() <= 5.0
+    assert (var >= 0.0).all()
+    # later targets condition mostly on earlier simulated ones
+    assert o.sim_nnear[:, 1].mean() > 15
+
+
+def test_sgsim_first_target_is_ordinary_kriging():
+    """The first visited target sees only the observations: with a zero draw
+    its value and variance are the ordinary-kriging estimate and variance."""
+    path = pd.read_csv(golden("path4800.csv"))["randpath"].values
+    o, pc, gr = _sgsim_pc2d(path, np.zeros(len(path)))
+    first = path[0] - 1
+    k = OracleKriging(ndim=2, nvar=1)
+    k.set_obs(1, pc[["x", "y"]].values, pc["pc"].values, nmax=20)
+    k.set_vgm(1, 1, **_VGM_PC2D)
+    k.set_grid(gr[["x", "y"]].values[first:first + 1])
+    k.set_search(1)
+    e, v = k.solve().get_results()
+    sims, var = o.get_results()
+    assert abs(sims[first] - e[0]) <= 1e-12 * max(1.0, abs(e[0]))
+    assert abs(var[first] - v[0]) <= 1e-12
+    assert o.sim_nnear[first, 1] == 0
+
+
+def test_sgsim_grid_on_observations():
+    """tests/test_sgsim.py::test_grid_on_observations_no_nan: targets at the
+    data reproduce them (co-located simulated targets are dropped)."""
+    rng = np.random.default_rng(3)
+    coord = rng.uniform(0.0, 100.0, size=(12, 2))
+    value = np.exp(rng.normal(0.0, 1.0, size=12))
+    o = OracleKriging(ndim=2, nvar=1, nsim=1)
+    o.set_obs(1, coord, value, nmax=12)
+    o.set_grid(coord.copy())
+    o.set_vgm(1, 1, "sph", nugget=0.0, sill=1.0, a_major=40.0)
+    o.set_search(1)
+    o.set_sim(np.arange(1, 13), rng.normal(0, 1, 12))
+    est, _ = o.solve().get_results()
+    assert np.isnan(est).sum() == 0
+    np.testing.assert_allclose(est, value, rtol=1e-2, atol=1e-2)
