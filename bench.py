@@ -14,7 +14,9 @@ same measurement for the FP64 form and ``auto_default`` for the library's
 default precision (per neighbour-count list the faster form, as timed by the
 kernel tuner); ``replay`` times the weight-store re-estimate (store_weight
 solve once, then update_obs_value + solve per step: one gather-dot kernel);
-``e2e`` is the same metric through the
+``sgsim`` times a sequential Gaussian simulation (four realisations on a
+200 x 200 grid) against the oracle's sequential run; ``e2e`` is the same
+metric through the
 public ``Kriging`` API with host inputs/outputs copied every step.  The
 reference arm (``--impl reference``) times the CPU restatement of the
 reference engine (oracle/kk_oracle.c, OpenMP over all host threads) on a
@@ -227,6 +229,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-auto", action="store_true", help="skip the leg of the default precision (auto)")
     ap.add_argument("--no-replay", action="store_true", help="skip the weight-store re-estimate leg")
+    ap.add_argument("--no-sgsim", action="store_true", help="skip the sequential-simulation leg")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
                     help="form of the timed leg (fp64 is for profiling the plain form alone)")
     args = ap.parse_args()
@@ -385,6 +388,56 @@ def main():
         kr.close()
         del kr
 
+    # ---- sequential Gaussian simulation: config 1's observations, a 200 x 200
+    # grid, nmax 24, four realisations along a seeded path (rank 0, one GPU)
+    sgsim = None
+    if not args.no_sgsim and rank == 0 and not W.st:
+        from krigekit_b200 import Kriging
+        w1 = bw.config1(grid_n=200)
+        ob = w1["obs"][0]
+        rng = np.random.default_rng(9)
+        sg = w1["grid"]
+        path = rng.permutation(len(sg)) + 1
+        nsim_b = 4
+        smp = rng.normal(0, 1, (len(sg), nsim_b))
+        spec = w1["vgm"][0][2]
+
+        def sg_setup(k):
+            k.set_obs(1, ob["coord"], ob["value"], nmax=24)
+            k.set_vgm(1, 1, **spec)
+            k.set_grid(sg)
+            k.set_search(1)
+            k.set_sim(path, smp)
+            return k
+
+        ks = sg_setup(Kriging(ndim=2, nvar=1, nsim=nsim_b, seed=3))
+        ks.solve()
+        ks.profile(True)
+        sg_ms = []
+        for _ in range(max(1, args.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ks.solve()
+            e1.record()
+            e1.synchronize()
+            sg_ms.append(e0.elapsed_time(e1))
+        sims_g, _ = ks.get_results()
+        sgsim = {"value": len(sg) * nsim_b / (statistics.median(sg_ms) / 1e3), "unit": "simulated values/s",
+                 "ms_per_solve": statistics.median(sg_ms), "targets": len(sg), "nsim": nsim_b, "nmax": 24,
+                 "phases_ms": ks.phases(), "workload": "config-1 observations, 200 x 200 grid, sph, seeded path"}
+        if not args.no_cpu:
+            from oracle.oracle import OracleKriging
+            ko = sg_setup(OracleKriging(ndim=2, nvar=1, nsim=nsim_b))
+            t0 = time.perf_counter()
+            ko.solve()
+            tcpu = time.perf_counter() - t0
+            so, _ = ko.get_results()
+            sgsim["cpu_oracle"] = {"value": len(sg) * nsim_b / tcpu, "seconds": tcpu, "cores": 1,
+                                   "kind": "port (sequential, as the reference runs SGSIM)"}
+            sgsim["max_abs_diff_vs_oracle"] = float(np.nanmax(np.abs(np.asarray(sims_g) - so)))
+        ks.close()
+        del ks
+
     # ---- roofline of the dominant kernel (the factorisation kernels)
     peaks = measured_peaks(torch, dev)
     p_aug, q_rhs = W.pq()
@@ -470,6 +523,7 @@ def main():
             "speedup_fp32r_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "auto_default": auto,
             "replay": replay,
+            "sgsim": sgsim,
             "kernel_plan": k32_plan,
             "accuracy": acc,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",

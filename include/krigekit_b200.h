@@ -35,9 +35,10 @@ int krige_ind_set_ncat(int64_t handle, int ncat);
 int krige_destroy(int64_t *handle);
 
 /* kriging_capi.F90:143-192 krige_initialize -> initialize_base (kriging_base.F90:467-553).
- * nsim > 0, weight_correction, varying_vgm and a non-empty weight_file are outside the
- * GPU kriging path and return an error; store_weight / use_old_weight select the
- * in-memory weight store (below). */
+ * nsim > 0 selects sequential Gaussian simulation (krige_set_sim; one variable; seed seeds
+ * the draws when the caller gives none); weight_correction, varying_vgm and a non-empty
+ * weight_file are outside the GPU path and return an error; store_weight / use_old_weight
+ * select the in-memory weight store (below). */
 int krige_initialize(int64_t handle, int ndim, int nvar, int ndrift, int unbias, int nsim,
                      int anisotropic_search, int weight_correction, int use_old_weight,
                      int store_weight, int cross_validation, int write_mat, int neglect_error,
