@@ -130,6 +130,10 @@ int krige_get_estimate(int64_t handle, int nsim_c, int nblocks, double *out);
  * One variable, point targets, no sector search or external drift. */
 int krige_set_sim(int64_t handle, int nblocks, const int *randpath, int nsim_c, int nvar_c,
                   const double *sample);
+/* No counterpart in the reference.  Neighbour sets of the last sequential simulation:
+ * nnear(2, nblocks) = observation and simulated members; inear(mmax, nblocks), 0-based, in
+ * each target's system order: observations (< nobs), then nobs + visiting position. */
+int krige_get_sim_neighbours(int64_t handle, int nblocks, int mmax, int *nnear, int *inear);
 /* kriging_capi_common.F90:323-344 krige_get_estimate_all: out(nblocks, nvar_c, nsim_c). */
 int krige_get_estimate_all(int64_t handle, int nblocks, int nvar_c, int nsim_c, double *out);
 /* kriging_capi_common.F90:352-369 krige_get_variance: out(nblocks), variable 1. */

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(128, 2)
               for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
             }
             v = dadd(0.0, dmul(fast_cov<0>(P, zr, lag), 1.0));
+            if (v != v) v = rhs_cov_row(P, t, xr, vr, k - pa, rs);  // a table argument at a zone edge
           } else {
             v = rhs_cov_row(P, t, xr, vr, k - pa, rs);
           }

@@ -648,6 +648,25 @@ int krige_get_estimate(int64_t h, int nsim_c, int nblocks, double* out) {
   return krige_get_estimate_all(h, nblocks, 1, nsim_c, out);
 }
 
+// Neighbour sets of the last sequential simulation (extension): nnear(2, nblocks) =
+// observation and simulated members, inear(mmax, nblocks) 0-based in the order of each
+// target's system: observations (< nobs), then nobs + visiting position.
+int krige_get_sim_neighbours(int64_t h, int nblocks, int mmax, int* nnear, int* inear) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  check_solved(e);
+  if (e->nsim <= 0 || e->sim_nn.empty()) throw std::string("no sequential simulation has been solved");
+  if (nblocks != e->nblock) throw std::string("nblocks must match the solved blocks");
+  if (mmax < e->sim_mmax) throw std::string("mmax is smaller than the simulation's neighbour capacity");
+  std::memcpy(nnear, e->sim_nn.data(), sizeof(int) * e->sim_nn.size());
+  for (int t = 0; t < nblocks; ++t) {
+    const int n = e->sim_nn[(size_t)t * 2] + e->sim_nn[(size_t)t * 2 + 1];
+    for (int i = 0; i < mmax; ++i) inear[(size_t)t * mmax + i] = i < n ? e->sim_nbr[(size_t)t * e->sim_mmax + i] : 0;
+  }
+  KK_GUARD_END
+}
+
 // krige_set_sim, kriging_capi.F90:410-443 -> set_sim_base (kriging_base.F90:1226-1320):
 // randpath (nblocks, 1-based) and sample (nsim, nvar, nblocks), either may be NULL
 int krige_set_sim(int64_t h, int nblocks, const int* randpath, int nsim_c, int nvar_c, const double* sample) {

@@ -1425,6 +1425,17 @@ static void engine_sgsim(Engine& e) {
   KK_CUDA(cudaMemcpyAsync(hn.data(), s.vd[0].nnear.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
   KK_CUDA(cudaMemcpyAsync(hl.data(), s.vd[0].nbr.p, sizeof(int) * hl.size(), cudaMemcpyDeviceToHost, st));
   KK_CUDA(cudaStreamSynchronize(st));
+  e.sim_mmax = mm;
+  e.sim_nn.assign((size_t)nb * 2, 0);
+  e.sim_nbr.assign((size_t)nb * mm, 0);
+  for (int p = 0; p < nb; ++p) {
+    const int t = e.sim_path[p] - 1;
+    int no = 0;
+    for (int i = 0; i < hn[p]; ++i) no += hl[(size_t)p * mm + i] < nobs;
+    e.sim_nn[(size_t)t * 2] = no;
+    e.sim_nn[(size_t)t * 2 + 1] = hn[p] - no;
+    std::memcpy(&e.sim_nbr[(size_t)t * mm], &hl[(size_t)p * mm], sizeof(int) * hn[p]);
+  }
   std::vector<int> lev(nb, 0);
   int nlev = 0;
   for (int p = 0; p < nb; ++p) {

@@ -152,6 +152,11 @@ struct Engine {
   std::vector<double> sim_sample;
   int sim_nobs = -1;
   int sim_levels = 0;  // dependency levels of the last simulation
+  // neighbour sets of the last simulation by target: counts (observation,
+  // simulated) and lists (sim_mmax per target; observations < nobs, then
+  // nobs + visiting position), in the order of the target's system
+  int sim_mmax = 0;
+  std::vector<int> sim_nn, sim_nbr;
 
   int naug() const { return std_ck ? unbias * nvar : unbias; }
   int pdrift() const { return ndrift + naug(); }

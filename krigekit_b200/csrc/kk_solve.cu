@@ -46,6 +46,12 @@ void set_zones(cudaStream_t st) {
     o += n;
   }
   for (int k = 0; k < 4; ++k) z.zb[k] = hb[k];
+  // the fast paths' compile-time copy of these zones (load_zones)
+  const ZoneRegs c = load_zones_host();
+  if (z.zn[0] != c.n0 || z.zn[1] != c.n1 || z.zn[2] != c.n2 || z.off[1] != c.o1 || z.off[2] != c.o2 ||
+      z.inv_dh[0] != c.i0 || z.inv_dh[1] != c.i1 || z.inv_dh[2] != c.i2 || z.zb[1] != c.zb1 || z.zb[2] != c.zb2 ||
+      z.zb[3] != c.zb3)
+    throw std::string("covariance table zones differ from the fast paths' constants");
   cudaMemcpyToSymbolAsync(c_zones, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
 }
 

@@ -207,25 +207,44 @@ __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 
 // zone constants of the lookup tables, held in registers
 struct ZoneRegs {
-  double zb1, zb2, zb3, i0, i1, i2;
+  double zb1, zb2, zb3, zb3e, i0, i1, i2;
   int o1, o2, n0, n1, n2;
 };
 
-__device__ __forceinline__ ZoneRegs load_zones() {
+// The reference's lookup clamps the index to a zone's last cell but keeps
+// the fraction of the unclamped index (variogram.f90:369-373), so a distance
+// a few ulp below a zone's end whose index rounds up to the zone size reads
+// one cell early.  The fast paths compute h to a few ulp of the reference's
+// h: a table argument within 1e-6 of a cell index from a zone's ends could
+// land on the other side, and the lookup returns NaN there so that the caller
+// takes the exact path.  zb3e: arguments up to just past the table's end
+// still go through the lookup (and its edge test).
+constexpr double KK_ZONE_EDGE = 1e-6;
+
+// The reference's zones are fixed (bounds 0, 0.1, 0.5, 3.5, steps 1e-5,
+// 1e-4, 1e-3: kriging.F90:416-417, alloc_zones in variogram.f90:223-256), so
+// the fast paths take them as compile-time constants, computed with the
+// same operations as set_zones (which checks that they agree), and hold no
+// registers for them.
+constexpr double KK_ZB1 = 0.1, KK_ZB2 = 0.5, KK_ZB3 = 3.5;
+constexpr int KK_ZN0 = 10000, KK_ZN1 = 4000, KK_ZN2 = 3000;
+__host__ __device__ __forceinline__ ZoneRegs load_zones_host() {
   ZoneRegs z;
-  z.zb1 = c_zones.zb[1];
-  z.zb2 = c_zones.zb[2];
-  z.zb3 = c_zones.zb[3];
-  z.i0 = c_zones.inv_dh[0];
-  z.i1 = c_zones.inv_dh[1];
-  z.i2 = c_zones.inv_dh[2];
-  z.o1 = c_zones.off[1];
-  z.o2 = c_zones.off[2];
-  z.n0 = c_zones.zn[0];
-  z.n1 = c_zones.zn[1];
-  z.n2 = c_zones.zn[2];
+  z.zb1 = KK_ZB1;
+  z.zb2 = KK_ZB2;
+  z.zb3 = KK_ZB3;
+  z.zb3e = KK_ZB3 * (1.0 + 1e-12);
+  z.i0 = (double)KK_ZN0 / (KK_ZB1 - 0.0);
+  z.i1 = (double)KK_ZN1 / (KK_ZB2 - KK_ZB1);
+  z.i2 = (double)KK_ZN2 / (KK_ZB3 - KK_ZB2);
+  z.o1 = KK_ZN0;
+  z.o2 = KK_ZN0 + KK_ZN1;
+  z.n0 = KK_ZN0;
+  z.n1 = KK_ZN1;
+  z.n2 = KK_ZN2;
   return z;
 }
+__device__ __forceinline__ ZoneRegs load_zones() { return load_zones_host(); }
 
 // tab_lookup without divergent constant-memory indexing: the same zone
 // choice, index and interpolation (variogram.f90:353-382, 682-710) from
@@ -237,6 +256,7 @@ __device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, cons
   const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
   const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
   double fi = dmul(dsub(h, lo), inv);
+  if (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)) return __longlong_as_double(0x7ff8000000000000ll);
   const int ii = (int)fi;
   const int i = off + min(ii, nm1);
   fi = dsub(fi, (double)ii);
@@ -288,7 +308,7 @@ template <int FM>  // 1 or 2 when known at compile time, 0: read P.fast_model
 __device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs& z, const double* lag) {
   const double h = aniso_h_fast(P.fm, P.fm_ndim, lag);
   if (FM == 1 || (FM == 0 && P.fast_model == 1)) {
-    if (h < z.zb3) return tab_fast(P.tables + P.fm_tab_off, z, h);
+    if (h < z.zb3e) return tab_fast(P.tables + P.fm_tab_off, z, h);
     return P.fm_tail ? tail_cov(P.models, h) : 0.0;
   }
   double res = 0.0;
@@ -297,7 +317,7 @@ __device__ __forceinline__ double fast_cov(const SolveParams& P, const ZoneRegs&
     if (s < P.fa_nst) {
       const double hs = P.fa_k[s] * h;
       double g;
-      if (hs < z.zb3) g = tab_fast(P.tables + P.fa_off[s], z, hs);
+      if (hs < z.zb3e) g = tab_fast(P.tables + P.fa_off[s], z, hs);
       else g = ((P.fa_tailmask >> s) & 1) ? tail_comp(&P.models[0].comp[s], hs) : 0.0;
       res = dadd(res, g);
     }
@@ -313,9 +333,9 @@ __device__ __forceinline__ double fast_cov_st(const SolveParams& P, const ZoneRe
   const double dt = P.ndim == 1 ? lag[1] : (P.ndim == 2 ? lag[2] : lag[3]);
   const double ht = fabs(P.ft_k * fabs(dt));
   double cs, ct;
-  if (hs < z.zb3) cs = tab_fast(P.tables + P.fm_tab_off, z, hs);
+  if (hs < z.zb3e) cs = tab_fast(P.tables + P.fm_tab_off, z, hs);
   else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
-  if (ht < z.zb3) ct = tab_fast(P.tables + P.ft_off, z, ht);
+  if (ht < z.zb3e) ct = tab_fast(P.tables + P.ft_off, z, ht);
   else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
   if (P.st_kind == 1) return dadd(dadd(dmul(dmul(P.st_kps, cs), ct), cs), ct);
   return dadd(cs, ct);
@@ -331,7 +351,7 @@ __device__ __forceinline__ double fast_cov_pair(const SolveParams& P, const Zone
   const int kind = P.fq_kind[pair];
   if (kind == 1) {
     const double hs = P.fq_k[pair][0] * h;
-    if (hs < z.zb3) return tab_fast(P.tables + P.fq_off[pair][0], z, hs);
+    if (hs < z.zb3e) return tab_fast(P.tables + P.fq_off[pair][0], z, hs);
     return (P.fq_tail[pair] & 1) ? tail_cov(P.models + pair, hs) : 0.0;
   }
   double res = 0.0;
@@ -342,7 +362,7 @@ __device__ __forceinline__ double fast_cov_pair(const SolveParams& P, const Zone
       const double hs = P.fq_k[pair][s] * h;
       double g;
       if (kind == 3) g = comp_cov_h(P.models[pair].comp[s], hs);
-      else if (hs < z.zb3) g = tab_fast(P.tables + P.fq_off[pair][s], z, hs);
+      else if (hs < z.zb3e) g = tab_fast(P.tables + P.fq_off[pair][s], z, hs);
       else g = ((P.fq_tail[pair] >> s) & 1) ? tail_comp(&P.models[pair].comp[s], hs) : 0.0;
       res = dadd(res, g);
     }
@@ -359,14 +379,16 @@ static __device__ __noinline__ double rhs_cov_row(const SolveParams& P, int t, c
       double node[4], lag[4];
       for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.gx[d][k]);
       make_lag(P, xr, node, rs, lag);
-      const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+      double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+      if (cv != cv) cv = cov_pair(P, vr, iv, lag);  // a table argument at a zone edge
       tmp = dadd(tmp, dmul(cv, __ldg(&P.gw[k])));
     }
   } else {
     double node[4], lag[4];
     for (int d = 0; d < P.nlag; ++d) node[d] = __ldg(&P.tx[d][t]);
     make_lag(P, xr, node, rs, lag);
-    const double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+    double cv = P.fast_model == 4 ? fast_cov_st(P, load_zones(), lag) : cov_pair(P, vr, iv, lag);
+    if (cv != cv) cv = cov_pair(P, vr, iv, lag);  // a table argument at a zone edge
     tmp = dadd(tmp, dmul(cv, 1.0));
   }
   return tmp;
@@ -392,6 +414,7 @@ __device__ __forceinline__ double tab_h(const double2* __restrict__ tab, const Z
   const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
   const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
   double fi = (h - lo) * inv;
+  if (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)) return __longlong_as_double(0x7ff8000000000000ll);
   const int ii = (int)fi;
   fi -= (double)ii;
   const double2 t = __ldg(&tab[off + min(ii, nm1)]);
@@ -413,7 +436,7 @@ template <int FM>
 __device__ __forceinline__ double cov_h(const SolveParams& P, const ZoneRegs& z, double h, const PairModel* pm,
                                         int pair) {
   if (FM == 1) {
-    if (h < z.zb3) return tab_h(P.tables + P.fm_tab_off, z, h);
+    if (h < z.zb3e) return tab_h(P.tables + P.fm_tab_off, z, h);
     return P.fm_tail ? tail_cov(P.models, h) : 0.0;
   }
   if (FM == 2) {
@@ -423,7 +446,7 @@ __device__ __forceinline__ double cov_h(const SolveParams& P, const ZoneRegs& z,
       if (s < P.fa_nst) {
         const double hs = P.fa_k[s] * h;
         double g;
-        if (hs < z.zb3) g = tab_h(P.tables + P.fa_off[s], z, hs);
+        if (hs < z.zb3e) g = tab_h(P.tables + P.fa_off[s], z, hs);
         else g = ((P.fa_tailmask >> s) & 1) ? tail_comp(&P.models[0].comp[s], hs) : 0.0;
         res += g;
       }
@@ -433,7 +456,7 @@ __device__ __forceinline__ double cov_h(const SolveParams& P, const ZoneRegs& z,
   const PairModel& m = pm[pair];
   if (m.kind == 1) {
     const double hs = m.k[0] * h;
-    if (hs < z.zb3) return tab_h(P.tables + m.off[0], z, hs);
+    if (hs < z.zb3e) return tab_h(P.tables + m.off[0], z, hs);
     return (m.tail & 1) ? tail_cov(P.models + pair, hs) : 0.0;
   }
   double res = 0.0;
@@ -443,7 +466,7 @@ __device__ __forceinline__ double cov_h(const SolveParams& P, const ZoneRegs& z,
       const double hs = m.k[s] * h;
       double g;
       if (m.kind == 3) g = comp_cov_h(P.models[pair].comp[s], hs);
-      else if (hs < z.zb3) g = tab_h(P.tables + m.off[s], z, hs);
+      else if (hs < z.zb3e) g = tab_h(P.tables + m.off[s], z, hs);
       else g = ((m.tail >> s) & 1) ? tail_comp(&P.models[pair].comp[s], hs) : 0.0;
       res += g;
     }
@@ -456,9 +479,9 @@ __device__ __forceinline__ double cov_h(const SolveParams& P, const ZoneRegs& z,
 __device__ __forceinline__ double cov_st_h(const SolveParams& P, const ZoneRegs& z, double hs, double dt) {
   const double ht = fabs(P.ft_k * fabs(dt));
   double cs, ct;
-  if (hs < z.zb3) cs = tab_h(P.tables + P.fm_tab_off, z, hs);
+  if (hs < z.zb3e) cs = tab_h(P.tables + P.fm_tab_off, z, hs);
   else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
-  if (ht < z.zb3) ct = tab_h(P.tables + P.ft_off, z, ht);
+  if (ht < z.zb3e) ct = tab_h(P.tables + P.ft_off, z, ht);
   else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
   if (P.st_kind == 1) return P.st_kps * cs * ct + cs + ct;
   return cs + ct;

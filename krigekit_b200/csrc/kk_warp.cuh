@@ -209,6 +209,16 @@ __global__ void __launch_bounds__(256, 3) k_assemble(const __grid_constant__ Sol
         const double hh = fd == 1 ? fabs(d0) : sqrt_newton(h2);
         kv = FM == 4 ? cov_st_h(P, zr, hh, s.x[nsp][c] - s.x[nsp][r])
                      : cov_h<FM == 4 ? 1 : FM>(P, zr, hh, s_pm, FM == 3 ? vr * 2 + s.var[c] : 0);
+        if (kv != kv) {  // a table argument at a zone edge: the reference's arithmetic
+          double lag[4];
+#pragma unroll
+          for (int d = 0; d < 4; ++d) lag[d] = d < P.nlag ? dsub(s.x[d][c], s.x[d][r]) : 0.0;
+          if (scale_lag) {
+#pragma unroll
+            for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
+          }
+          kv = cov_pair_call(P, vr, s.var[c], lag[0], lag[1], lag[2], lag[3]);
+        }
       } else {
         double lag[4];
 #pragma unroll
@@ -325,6 +335,7 @@ __global__ void __launch_bounds__(32 * warp_cta<T, N, REFINE>(), warp_min_ctas<T
                 for (int d = 0; d < 4; ++d) lag[d] = lag[d] / rs;
               }
               v = dadd(0.0, dmul(fast_cov<0>(P, zr, lag), 1.0));
+              if (v != v) v = rhs_cov_row(P, t, xr, vr, iv, rs);  // a table argument at a zone edge
             } else {
               v = rhs_cov_row(P, t, xr, vr, iv, rs);
             }

@@ -330,6 +330,17 @@ class Kriging:
         _lib.call("krige_set_sim", self._h(), nblocks, rp_ptr, nsim_c, nvar_c, s_ptr)
         self._set_sim = True
 
+    def get_sim_neighbours(self, mmax: int):
+        """Neighbour sets of the last sequential simulation (extension;
+        krige_get_sim_neighbours): (nnear (nblocks, 2) observation and
+        simulated members, inear (nblocks, mmax) 0-based in system order:
+        observations < nobs, then nobs + visiting position)."""
+        nb = self._nb()
+        nn = np.zeros((nb, 2), dtype=np.int32)
+        inear = np.zeros((nb, mmax), dtype=np.int32)
+        _lib.call("krige_get_sim_neighbours", self._h(), nb, int(mmax), _iptr(nn), _iptr(inear))
+        return nn, inear
+
     def solve(self, nthread: int = 0, ncache: Optional[int] = None):
         """Run the kriging solve on the GPU (kriging.py:1321-1344)."""
         _lib.call("krige_solve", self._h(), int(nthread), -1 if ncache is None else int(ncache))

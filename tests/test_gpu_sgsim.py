@@ -17,6 +17,7 @@ import numpy as np
 import pandas as pd
 import pytest
 
+import bench_workloads as bw
 from conftest import golden
 from oracle.oracle import OracleKriging
 
@@ -48,6 +49,11 @@ def _pair(obs, z, grid, vgm, nsim, path, sample, nmax=20, search=None, obs_kw=No
 
 
 def _check(g, o, zspread, nsim):
+    nn, inear = g.get_sim_neighbours(o.sim_inear.shape[1])
+    np.testing.assert_array_equal(nn, o.sim_nnear)  # observation and simulated members per target
+    for t in range(len(nn)):
+        k = int(nn[t].sum())
+        assert np.array_equal(inear[t, :k], o.sim_inear[t, :k]), f"target {t}"  # system order too
     e, v = g.get_results(squeeze=False)
     oe, ov = o.get_results(squeeze=False)
     e = np.asarray(e).reshape(len(ov), nsim)
@@ -159,3 +165,20 @@ def test_sgsim_errors():
         k2.set_sim()
     with pytest.raises(RuntimeError, match="mutually exclusive"):
         Kriging(ndim=2, nvar=1, nsim=1, cross_validation=True)
+
+
+def test_sgsim_lattice_at_table_zone_edges():
+    """A 200 x 200 lattice of targets with a spherical range of 50 cells:
+    targets 5 cells apart sit at 0.1 of the range, the end of the first
+    table zone, where the reference's lookup reads one cell early (the
+    fraction of an unclamped index); the GPU's fast covariance must take the
+    reference's arithmetic there."""
+    w1 = bw.config1(grid_n=200)
+    ob = w1["obs"][0]
+    rng = np.random.default_rng(9)
+    grid = w1["grid"]
+    path = rng.permutation(len(grid)) + 1
+    sample = rng.normal(0, 1, (len(grid), 2))
+    vgm = w1["vgm"][0][2]
+    g, o = _pair(ob["coord"], ob["value"], grid, vgm, 2, path, sample, nmax=24)
+    _check(g, o, float(np.ptp(ob["value"])), 2)
