@@ -48,8 +48,8 @@ METRIC = "kriged targets/s on 1 B200: FP32+refine batched vs FP64 plain at <=1e-
 # chunk (its traffic is the chunk's K64 read back, 16.6 KB per target), the
 # search launch all 160 000 targets (coordinates and neighbour lists); both
 # grow in proportion to the targets.
-NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (1096.717e6 + 22.697e6) / 65536,
-                             "search": (8.633e6 + 1.268e6) / 160000}
+NCU_DRAM_BYTES_PER_TARGET = {"solve_fp32_refine": (1098.960e6 + 30.646e6) / 65536,
+                             "search": (8.722e6 + 1.375e6) / 160000}
 
 
 def solve_flops(n, p=1, q=1):
