@@ -230,6 +230,9 @@ def main():
     ap.add_argument("--no-auto", action="store_true", help="skip the leg of the default precision (auto)")
     ap.add_argument("--no-replay", action="store_true", help="skip the weight-store re-estimate leg")
     ap.add_argument("--no-sgsim", action="store_true", help="skip the sequential-simulation leg")
+    ap.add_argument("--autotune", type=int, default=None, choices=[0, 1, 2],
+                    help="kernel plan: 0 fixed (use under a profiler, whose serialised launches distort the "
+                         "tuner's timings), 1 tuned once per signature (the library default)")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
                     help="form of the timed leg (fp64 is for profiling the plain form alone)")
     args = ap.parse_args()
@@ -255,6 +258,7 @@ def main():
     dev = torch.cuda.current_device()
 
     W = bw.Workload(args.config, args.grid, args.nmax)
+    W.autotune = args.autotune
     w = W.w
     nvar = w["nvar"]
     ntarget = W.ntarget

@@ -269,6 +269,8 @@ class Workload:
     def ndim(self):
         return self.w["ndim"]
 
+    autotune = None  # kernel plan of the product objects (None: the library default)
+
     def product(self, precision, nmin=None, idx=None, **extra):
         from krigekit_b200 import Kriging, SpaceTimeKriging
         nmin = self.w["nmin"] if nmin is None else nmin
@@ -277,6 +279,8 @@ class Workload:
         else:
             k = Kriging(ndim=self.w["ndim"], nvar=self.w["nvar"], precision=precision, nmin=nmin, **self.w["kw"],
                         **extra)
+        if self.autotune is not None:
+            k.set_autotune(self.autotune)
         return self.configure(k, idx)
 
     def oracle(self, nmin=None, idx=None):

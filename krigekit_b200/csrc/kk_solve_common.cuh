@@ -249,6 +249,10 @@ __device__ __forceinline__ ZoneRegs load_zones() { return load_zones_host(); }
 // tab_lookup without divergent constant-memory indexing: the same zone
 // choice, index and interpolation (variogram.f90:353-382, 682-710) from
 // register selects.  Valid for 0 <= h < zb3.
+// EDGE: the argument comes from a fast h (a few ulp from the reference's),
+// so zone ends return NaN; arguments computed exactly as the reference does
+// (the temporal |k_t dt|) read the table as it is.
+template <bool EDGE = true>
 __device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, const ZoneRegs& z, double h) {
   const bool z0 = h < z.zb1, z1 = h < z.zb2;
   const double lo = z0 ? 0.0 : (z1 ? z.zb1 : z.zb2);
@@ -256,7 +260,8 @@ __device__ __forceinline__ double tab_fast(const double2* __restrict__ tab, cons
   const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
   const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
   double fi = dmul(dsub(h, lo), inv);
-  if (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)) return __longlong_as_double(0x7ff8000000000000ll);
+  if (EDGE && (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)))
+    return __longlong_as_double(0x7ff8000000000000ll);
   const int ii = (int)fi;
   const int i = off + min(ii, nm1);
   fi = dsub(fi, (double)ii);
@@ -335,7 +340,7 @@ __device__ __forceinline__ double fast_cov_st(const SolveParams& P, const ZoneRe
   double cs, ct;
   if (hs < z.zb3e) cs = tab_fast(P.tables + P.fm_tab_off, z, hs);
   else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
-  if (ht < z.zb3e) ct = tab_fast(P.tables + P.ft_off, z, ht);
+  if (ht < z.zb3) ct = tab_fast<false>(P.tables + P.ft_off, z, ht);  // |k_t dt| as the reference forms it
   else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
   if (P.st_kind == 1) return dadd(dadd(dmul(dmul(P.st_kps, cs), ct), cs), ct);
   return dadd(cs, ct);
@@ -407,6 +412,7 @@ __device__ __forceinline__ double sqrt_newton(double h2) {
 
 // table value at h, 0 <= h < zb3: the zone, index and linear interpolation
 // of the reference's lookup (variogram.f90:353-382, 682-710)
+template <bool EDGE = true>
 __device__ __forceinline__ double tab_h(const double2* __restrict__ tab, const ZoneRegs& z, double h) {
   const bool z0 = h < z.zb1, z1 = h < z.zb2;
   const double lo = z0 ? 0.0 : (z1 ? z.zb1 : z.zb2);
@@ -414,7 +420,8 @@ __device__ __forceinline__ double tab_h(const double2* __restrict__ tab, const Z
   const int off = z0 ? 0 : (z1 ? z.o1 : z.o2);
   const int nm1 = (z0 ? z.n0 : (z1 ? z.n1 : z.n2)) - 1;
   double fi = (h - lo) * inv;
-  if (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)) return __longlong_as_double(0x7ff8000000000000ll);
+  if (EDGE && (fi > (double)(nm1 + 1) - KK_ZONE_EDGE || (!z0 && fi < KK_ZONE_EDGE)))
+    return __longlong_as_double(0x7ff8000000000000ll);
   const int ii = (int)fi;
   fi -= (double)ii;
   const double2 t = __ldg(&tab[off + min(ii, nm1)]);
@@ -481,7 +488,7 @@ __device__ __forceinline__ double cov_st_h(const SolveParams& P, const ZoneRegs&
   double cs, ct;
   if (hs < z.zb3e) cs = tab_h(P.tables + P.fm_tab_off, z, hs);
   else cs = P.fm_tail ? tail_cov(&P.smodels[0].cs, hs) : 0.0;
-  if (ht < z.zb3e) ct = tab_h(P.tables + P.ft_off, z, ht);
+  if (ht < z.zb3) ct = tab_h<false>(P.tables + P.ft_off, z, ht);  // |k_t dt| as the reference forms it
   else ct = P.ft_tail ? tail_cov(&P.smodels[0].ct, ht) : 0.0;
   if (P.st_kind == 1) return P.st_kps * cs * ct + cs + ct;
   return cs + ct;
