@@ -4,8 +4,9 @@ It re-solves the neighbour sets of the last krige_solve with the generic
 one-thread-per-target kernel whose workspace, work list and counters live in
 a fixed static device array.  Each case calls it twice in a row with new
 observation values and compares both results with the existing entry points
-(krige_update_obs_value + krige_solve in FP64) on a second handle, and
-checks that the torch caching allocator saw no allocation during the calls.
+(krige_update_obs_value + krige_solve in FP64) on a second handle and with
+the oracle's solve of the same values, and checks that the torch caching
+allocator saw no allocation during the calls.
 This file is collected last so that it also runs after every other GPU test.
 """
 import ctypes
@@ -67,6 +68,32 @@ def _allocations():
     return torch.cuda.memory_stats().get("allocation.all.allocated", 0)
 
 
+def _vs_oracle(a, w, zstd, sill, what):
+    """The re-solve's results against the oracle's solve of workload w."""
+    from oracle.oracle import OracleKriging, OracleSpaceTime
+    if w.get("st"):
+        o = bw.apply_st(OracleSpaceTime(ndim=2), w)
+    else:
+        o = bw.apply(OracleKriging(ndim=w["ndim"], nvar=w["nvar"], **w["kw"]), w)
+    o.solve()
+    oe, ov = (np.array(x) for x in o.get_results(squeeze=False))
+    e_s, v_s = _results(a)
+    e_s = e_s.reshape(oe.shape)
+    v_s = v_s.reshape(ov.shape)
+    ok = ~np.isnan(oe)
+    assert np.array_equal(np.isnan(e_s), np.isnan(oe)), what
+    ee = np.nanmax(bw.rel_err(e_s[ok], oe[ok], 1e-3 * zstd))
+    ve = np.nanmax(bw.rel_err(v_s, ov, 1e-3 * sill))
+    assert ee <= TOL, f"{what}: estimate rel err {ee:.3e} against the oracle"
+    assert ve <= TOL, f"{what}: variance rel err {ve:.3e} against the oracle"
+
+
+def _with_values(w, ivar, znew):
+    obs = [dict(o) for o in w["obs"]]
+    obs[ivar - 1]["value"] = znew
+    return dict(w, obs=obs)
+
+
 def _check_two_calls(w, ivar):
     from krigekit_b200 import _lib
     a, b = _handle_pair(w)
@@ -85,6 +112,7 @@ def _check_two_calls(w, ivar):
         b.solve()
         _compare(a, b, float(np.std(znew)), w["sill"], f"call {call}")
         assert a.gpu_counters()["fail"] == 0
+        _vs_oracle(a, _with_values(w, ivar, znew), float(np.std(znew)), w["sill"], f"call {call}")
     # null values: the same neighbour sets and values give the same results again
     e1, v1 = _results(a)
     assert _resolve_static(a, 0, None) == 0, _lib.last_error()
@@ -121,6 +149,7 @@ def test_resolve_static_external_drift_changed_between_calls():
         assert _resolve_static(a, 0, None) == 0, _lib.last_error()
         b.solve()
         _compare(a, b, w["zstd"], w["sill"], f"drift call {call}")
+        _vs_oracle(a, dict(w, grid_drift=gd), w["zstd"], w["sill"], f"drift call {call}")
     a.close()
     b.close()
 
@@ -145,6 +174,8 @@ def test_resolve_static_after_set_vgm():
         assert _resolve_static(a, 0, None) == 0, _lib.last_error()
         b.solve()
         _compare(a, b, w["zstd"], sill + 0.05, f"vgm call {call}")
+        vgm = [(1, 1, dict(vtype="sph", nugget=0.05, sill=sill, a_major=rng_))]
+        _vs_oracle(a, dict(w, vgm=vgm), w["zstd"], sill + 0.05, f"vgm call {call}")
     a.close()
     b.close()
 
