@@ -14,6 +14,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kk_host.h"
@@ -53,10 +54,53 @@ static Engine* get(int64_t h) {
 
 static int ierr() { return failed() ? 1 : 0; }
 
+// Host memcpy of a large array split over threads: a caller's freshly
+// allocated output pages are first touched here, and one core faults them in
+// at a few GB/s.
+static void par_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPiece = size_t(4) << 20;
+  const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({size_t(8), size_t(hc), bytes / kPiece});
+  if (nt <= 1) {
+    if (bytes) std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t per = ((bytes + nt - 1) / nt + 63) & ~size_t(63);
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (size_t i = 1; i < nt; ++i) {
+    const size_t lo = i * per;
+    if (lo >= bytes) break;
+    const size_t n = std::min(per, bytes - lo);
+    th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, n); });
+  }
+  std::memcpy(dst, src, std::min(per, bytes));
+  for (auto& t : th) t.join();
+}
+
 // device -> host copy of solve results, with the CUDA status checked
 static void copy_d2h(void* dst, const void* src, size_t bytes) {
   const cudaError_t err = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
   if (err != cudaSuccess) throw std::string("CUDA error ") + cudaGetErrorString(err) + " reading results";
+}
+
+static const double* results_to_host(Engine* e, const void* src, size_t n, std::vector<double>& fallback);
+
+// Device results straight into a caller's array: small ones by one copy,
+// large ones through the handle's pinned buffer (full-rate DMA) and a
+// threaded host copy instead of the driver's pageable staging.
+static void results_to_caller(Engine* e, double* out, const void* src, size_t n) {
+  if (sizeof(double) * n < (size_t(8) << 20)) {
+    copy_d2h(out, src, sizeof(double) * n);
+    return;
+  }
+  std::vector<double> fb;
+  const double* tmp = results_to_host(e, src, n, fb);
+  if (tmp == fb.data()) {
+    std::memcpy(out, tmp, sizeof(double) * n);
+    return;
+  }
+  par_copy(out, tmp, sizeof(double) * n);
 }
 
 // Device results of a multi-variable solve into host memory for reordering:
@@ -371,7 +415,7 @@ static bool stage_targets(Engine* e, const double* coord, size_t nval) {
     }
     e->hstage_bytes = need;
   }
-  if (need) std::memcpy(e->hstage, coord, need);
+  par_copy(e->hstage, coord, need);
   return true;
 }
 
@@ -630,7 +674,7 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
   }
   if (nv == 1) {
     // est is (nblock) on the device: copy the first column straight into out
-    copy_d2h(out, e->est.p, sizeof(double) * nblocks);
+    results_to_caller(e, out, e->est.p, (size_t)nblocks);
   } else {
     std::vector<double> fb;
     const double* tmp = results_to_host(e, e->est.p, (size_t)e->nblock * nv, fb);
@@ -716,7 +760,7 @@ int krige_get_variance_all(int64_t h, int nblocks, int nvar_c, double* out) {
     throw std::string("output dimensions exceed the solved blocks or variables");
   if (nblocks == 0 || nvar_c == 0) return 0;
   if (nv == 1) {
-    copy_d2h(out, e->var.p, sizeof(double) * nblocks);
+    results_to_caller(e, out, e->var.p, (size_t)nblocks);
   } else {
     std::vector<double> fb;
     const double* tmp = results_to_host(e, e->var.p, (size_t)e->nblock * nv * nv, fb);
