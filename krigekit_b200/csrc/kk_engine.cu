@@ -679,7 +679,7 @@ void engine_solve(Engine& e) {
       // observations and the targets visited before it (exact kd-tree order)
       if (S.mode != 0 && !d.tree_ready) build_tree(e, v);
       const int nthreads = std::max(1, std::min(nb, 32768));
-      const int stride = S.nmax + 2;
+      const int stride = (S.mode == 2 ? S.K : S.nmax) + 2;
       DBuf heaps;
       heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);
       timer.start();
@@ -1351,7 +1351,9 @@ static void engine_sgsim(Engine& e) {
   if (e.obs.empty() || e.obs[0].n == 0) throw std::string("Observations need to be set first.");
   if (e.nblock == 0) throw std::string("Grid needs to be set first.");
   ObsVar& o = e.obs[0];
-  if (o.sector) throw std::string("sector search in sequential simulation is not supported by the GPU library");
+  if (o.sector && !(o.nmax > 0 && o.nmax < o.n + e.nblock))
+    throw std::string("sector search in sequential simulation needs nmax below the number of observations plus "
+                      "targets (the search tree exists only then)");
   if (o.nmax > (int)(INT_MAX * 0.001)) throw std::string("`nmax` must be set for all observations for SGSIM.");
   validate(e);
   const int nb = e.nblock, D = e.nlag, nsim = e.nsim, nobs = o.n;

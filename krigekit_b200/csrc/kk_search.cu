@@ -1156,15 +1156,22 @@ __global__ void k_search_kdtree(KkSearch S, const int* __restrict__ list, const 
 }
 
 // Neighbours of the targets of a sequential simulation (search_neighbors,
-// simulation branch, kriging.F90:524-612), one thread per target: the
-// observation set here is the nobs observations followed by the targets in
-// visiting order, and target p may use the observations and the targets
-// visited before it (indices < nobs + p).  The nmax nearest of those
-// (kdtree2_n_nearest_maxidx, heap order), or all of them when nmax does not
-// cut; the simulated members are cut by maxdist and dropped when co-located
-// with an observation neighbour (relative tolerance 1e-6).  The list is the
-// observation members ascending, then the simulated members in heap order:
-// the reference's matrix order.  heaps holds nmax + 2 entries per thread.
+// simulation branch, kriging.F90:524-612, and its closing maxdist filter,
+// :660-661), one thread per target.  The observation set here is the nobs
+// observations followed by the targets in visiting order, and target p may
+// use the observations and the targets visited before it (indices < nobs +
+// p).  Candidates: with sector search (S.mode 2) the min(nobs + p, S.K)
+// nearest, sorted by distance (the tree is built with sort = sector_search,
+// kriging.F90:378-381) and passed through the sector filter (at most nmax
+// per sector, observations and targets alike, maxdist on both); otherwise
+// the nmax nearest in heap order (kdtree2_n_nearest_maxidx), or all of them
+// when nmax does not cut.  Then: the simulated members beyond maxdist go,
+// the simulated members co-located with an observation member (relative
+// tolerance 1e-6) go, and last the observation members beyond maxdist go.
+// The list is the observation members ascending, then the simulated members
+// in candidate order: the reference's matrix order.  heaps holds the
+// candidates plus two entries per thread; a rejected candidate is marked by
+// idx = -1.
 __global__ void k_search_sgsim(KkSearch S, int ntarget, int nobs, const double* __restrict__ t0,
                                const double* __restrict__ t1, const double* __restrict__ t2,
                                const double* __restrict__ ox0, const double* __restrict__ ox1,
@@ -1181,52 +1188,93 @@ __global__ void k_search_sgsim(KkSearch S, int ntarget, int nobs, const double* 
     else for (int d = 0; d < S.ndim; ++d) q[d] = x[d];
     int* out = nbr + (size_t)p * S.mmax;
     const int lim = nobs + p;
-    int no = 0, nb = 0;
-    // members: observations go to out[0 ..), simulated ones to h[1 ..) as (dis, index)
-    if (S.nmax < lim) {
-      kd_n_nearest(S.tree, q, S.nmax, h, lim);
-      for (int i = 1; i <= S.nmax; ++i) {
+    const bool all = S.mode != 2 && S.nmax >= lim;
+    // candidates h[1 .. nc]; with all, the simulated ones only (the
+    // observations are 0 .. nobs - 1)
+    int nc;
+    if (S.mode == 2) {
+      nc = min(lim, S.K);
+      kd_n_nearest(S.tree, q, nc, h, lim);
+      kd_heapsort(h, nc);
+      int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int i = 1; i <= nc; ++i) {  // apply_sector_filter, kriging.F90:1093-1154
         const int idx = h[i].idx;
-        if (idx < nobs) out[no++] = idx;
-        else h[1 + nb++] = h[i];
+        bool take = h[i].dis <= S.maxd2;
+        if (take) {
+          double pt[3], pr[3];
+          for (int d = 0; d < S.ndim; ++d) pt[d] = os[d][idx];
+          if (S.aniso) rotate_pt(S.rotmat, S.ndim, pt, pr);
+          else for (int d = 0; d < S.ndim; ++d) pr[d] = pt[d];
+          const double dx = dsub(pr[0], q[0]);
+          const double dy = S.ndim > 1 ? dsub(pr[1], q[1]) : 0.0;
+          const double dz = S.ndim == 3 ? dsub(pr[2], q[2]) : 0.0;
+          const int sec = (dx < 0.0 ? 1 : 0) + (dy < 0.0 ? 2 : 0) + (dz < 0.0 ? 4 : 0);
+          take = cnt[sec] < S.nmax;
+          if (take) cnt[sec]++;
+        }
+        if (!take) h[i].idx = -1;
       }
+    } else if (!all) {
+      nc = S.nmax;
+      kd_n_nearest(S.tree, q, nc, h, lim);
     } else {
-      for (int i = 0; i < nobs; ++i) out[no++] = i;
+      nc = p;
       for (int j = 0; j < p; ++j) {  // rotated_dists of the raw centres (rotation.f90:193-218)
         double diff[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
         for (int d = 0; d < S.ndim; ++d) diff[d] = dsub(os[d][nobs + j], q[d]);
         rotate_pt(S.rotmat, S.ndim, diff, r);
         double s2 = 0.0;
         for (int d = 0; d < S.ndim; ++d) s2 = dadd(s2, dmul(r[d], r[d]));
-        h[1 + nb].dis = s2;
-        h[1 + nb].idx = nobs + j;
-        ++nb;
+        h[1 + j].dis = s2;
+        h[1 + j].idx = nobs + j;
       }
     }
-    // maxdist on the simulated members (filter_by_maxlag, kriging_base.F90:2491-2505),
-    // then the ones co-located with an observation member (kriging.F90:584-609)
-    int keep = 0;
-    for (int i = 1; i <= nb; ++i) {
-      if (!(h[i].dis <= S.maxd2)) continue;
+    // the simulated members: maxdist (filter_by_maxlag, kriging_base.F90:2491-2505),
+    // then co-location with an observation member (kriging.F90:584-609)
+    for (int i = 1; i <= nc; ++i) {
       const int idx = h[i].idx;
+      if (idx < nobs) continue;  // an observation, or rejected
+      if (!(h[i].dis <= S.maxd2)) { h[i].idx = -1; continue; }
       bool dup = false;
-      for (int o = 0; o < no && !dup; ++o) {
+      const int no_all = all ? nobs : nc;
+      for (int o = 0; o < no_all && !dup; ++o) {
+        const int io = all ? o : h[1 + o].idx;
+        if (io < 0 || io >= nobs) continue;
         dup = true;
         for (int d = 0; d < S.ndim; ++d) {
-          const double xo = os[d][out[o]];
+          const double xo = os[d][io];
           if (fabs(os[d][idx] - xo) > 1.0e-6 * (1.0 + fabs(xo))) { dup = false; break; }
         }
       }
-      if (!dup) h[1 + keep++] = h[i];
+      if (dup) h[i].idx = -1;
     }
-    // isort of the observation members (kriging_base.F90:3510-3524)
-    for (int i = 1; i < no; ++i) {
-      int tmp = out[i], j = i - 1;
-      while (j >= 0 && out[j] > tmp) { out[j + 1] = out[j]; --j; }
-      out[j + 1] = tmp;
+    // the observation members within maxdist (kriging.F90:660-661), ascending
+    int no = 0;
+    if (all) {
+      for (int i = 0; i < nobs; ++i) {
+        double diff[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < S.ndim; ++d) diff[d] = dsub(os[d][i], q[d]);
+        rotate_pt(S.rotmat, S.ndim, diff, r);
+        double s2 = 0.0;
+        for (int d = 0; d < S.ndim; ++d) s2 = dadd(s2, dmul(r[d], r[d]));
+        if (s2 <= S.maxd2) out[no++] = i;
+      }
+    } else {
+      for (int i = 1; i <= nc; ++i) {
+        const int idx = h[i].idx;
+        if (idx >= 0 && idx < nobs && h[i].dis <= S.maxd2) out[no++] = idx;
+      }
+      // isort of the observation members (kriging_base.F90:3510-3524)
+      for (int i = 1; i < no; ++i) {
+        int tmp = out[i], j = i - 1;
+        while (j >= 0 && out[j] > tmp) { out[j + 1] = out[j]; --j; }
+        out[j + 1] = tmp;
+      }
     }
-    for (int i = 0; i < keep; ++i) out[no + i] = h[1 + i].idx;
-    nnear[p] = no + keep;
+    int k = no;
+    for (int i = 1; i <= nc; ++i)
+      if (h[i].idx >= nobs) out[k++] = h[i].idx;
+    nnear[p] = k;
   }
 }
 

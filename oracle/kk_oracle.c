@@ -1720,15 +1720,28 @@ done:
 int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int nsim, orc_sim_result *R) {
   R->err = 0;
   R->errmsg[0] = 0;
-  if (P->nvar != 1 || P->st || P->nblockpnt || P->sector[0] || P->ndrift > 0 || P->cross_validation) {
+  if (P->nvar != 1 || P->st || P->nblockpnt || P->ndrift > 0 || P->cross_validation) {
     R->err = 1;
-    snprintf(R->errmsg, 256, "sgsim: one variable, point targets, no sectors, drift or cross-validation");
+    snprintf(R->errmsg, 256, "sgsim: one variable, point targets, no drift or cross-validation");
     return 1;
   }
   const int nb = P->nblock, nobs = P->nobs[0], ndim = P->ndim, nlag = ndim;
   const int ntot = nobs + nb;
   int nmax = P->nmax[0];
   if (nmax <= 0 || nmax > ntot) nmax = ntot;
+  /* sector search: the sorted candidates of kdtree2_n_nearest_maxidx (the
+   * tree is built with sort = sector_search, kriging.F90:378-381) through
+   * apply_sector_filter; the tree exists only when nmax cuts (need_search,
+   * kriging.F90:362-363) */
+  const int sector = P->sector[0];
+  if (sector && ntot <= nmax) {
+    R->err = 1;
+    snprintf(R->errmsg, 256, "sgsim: sector search needs nmax below the observations plus targets");
+    return 1;
+  }
+  const int lim4 = (1 << ndim) * nmax * 4;
+  const int ncmax = sector ? (ntot < lim4 ? ntot : lim4) : nmax;
+  const int mcap = sector ? (1 << ndim) * nmax : nmax;
   orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
   c->p = P;
   c->nvar = 1;
@@ -1749,7 +1762,8 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
   double a2 = P->s_anis2[0] != 0.0 ? P->s_anis2[0] : 1.0;
   const int aniso = (fabs(a1 - 1.0) > ORC_EPSLON || fabs(a2 - 1.0) > ORC_EPSLON) && P->anisotropic_search;
   double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  if (aniso) orc_calc_rotmat(P->s_az[0], P->s_dip[0], P->s_plunge[0], a1, a2, rot);
+  /* the rotation exists only with the tree (need_search, kriging.F90:371-376) */
+  if (aniso && ntot > nmax) orc_calc_rotmat(P->s_az[0], P->s_dip[0], P->s_plunge[0], a1, a2, rot);
   const double maxd2 = P->maxdist[0] * P->maxdist[0];
 
   /* observations, then the targets in visiting order */
@@ -1767,11 +1781,12 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
   kd_tree tree;
   kd_create(&tree, sc, nlag, ntot);
   double *vals = (double *)malloc(sizeof(double) * (size_t)nsim * nb);  /* [isim][path position] */
-  kd_res *h = (kd_res *)malloc(sizeof(kd_res) * ((size_t)nmax + 1));
+  kd_res *h = (kd_res *)malloc(sizeof(kd_res) * ((size_t)ncmax + 1));
+  double *dob = (double *)malloc(sizeof(double) * ((size_t)ntot + 1));
   int *io = (int *)malloc(sizeof(int) * ((size_t)ntot + 1));
   int *ib_ = (int *)malloc(sizeof(int) * ((size_t)ntot + 1));
   double *db = (double *)malloc(sizeof(double) * ((size_t)ntot + 1));
-  const int mm = nmax + pa;
+  const int mm = mcap + pa;
   double *A = (double *)malloc(sizeof(double) * (size_t)mm * mm);
   double *B = (double *)malloc(sizeof(double) * mm);
   double *X = (double *)malloc(sizeof(double) * mm);
@@ -1795,14 +1810,44 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
     else for (int d = 0; d < ndim; ++d) newloc[d] = xloc[d];
     int no = 0, nbk = 0;
     const int lim = nobs + p;
-    if (nmax < lim) {
+    if (sector) {
+      const int ncand = lim < ncmax ? lim : ncmax;
+      kd_n_nearest_max(&tree, newloc, ncand, 1, h, lim);
+      /* apply_sector_filter, kriging.F90:1093-1154, over observations and
+       * earlier targets alike (obsloc holds both) */
+      int count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int i = 1; i <= ncand; ++i) {
+        const int idx = h[i].idx;
+        if (h[i].dis > maxd2) continue;
+        double pr[3];
+        if (aniso) rotate_pt(rot, ndim, xc + (size_t)idx * nlag, pr);
+        else for (int d = 0; d < ndim; ++d) pr[d] = xc[(size_t)idx * nlag + d];
+        const double dx = pr[0] - newloc[0];
+        const double dy = ndim > 1 ? pr[1] - newloc[1] : 0.0;
+        const double dz = ndim == 3 ? pr[2] - newloc[2] : 0.0;
+        const int sec = (dx < 0.0 ? 1 : 0) + (dy < 0.0 ? 2 : 0) + (ndim == 3 && dz < 0.0 ? 4 : 0);
+        if (count[sec] < nmax) {
+          count[sec]++;
+          if (idx < nobs) { dob[no] = h[i].dis; io[no++] = idx; }
+          else { ib_[nbk] = idx - nobs; db[nbk] = h[i].dis; ++nbk; }
+        }
+      }
+    } else if (nmax < lim) {
       kd_n_nearest_max(&tree, newloc, nmax, 0, h, lim);
       for (int i = 1; i <= nmax; ++i) {
-        if (h[i].idx < nobs) io[no++] = h[i].idx;
+        if (h[i].idx < nobs) { dob[no] = h[i].dis; io[no++] = h[i].idx; }
         else { ib_[nbk] = h[i].idx - nobs; db[nbk] = h[i].dis; ++nbk; }
       }
     } else {
-      for (int i = 0; i < nobs; ++i) io[no++] = i;
+      for (int i = 0; i < nobs; ++i) {  /* rotated_dists of the raw observations */
+        double diff[3], r[3];
+        for (int d = 0; d < ndim; ++d) diff[d] = xc[(size_t)i * nlag + d] - newloc[d];
+        rotate_pt(rot, ndim, diff, r);
+        double s2 = 0.0;
+        for (int d = 0; d < ndim; ++d) s2 = s2 + r[d] * r[d];
+        dob[no] = s2;
+        io[no++] = i;
+      }
       for (int q = 0; q < p; ++q) {  /* rotated_dists of the raw block centres (rotation.f90:193-218) */
         double diff[3], r[3];
         for (int d = 0; d < ndim; ++d) diff[d] = xc[(size_t)(nobs + q) * nlag + d] - newloc[d];
@@ -1836,6 +1881,12 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
       }
       nbk = k2;
     }
+    /* filter_by_maxlag on the observation group (kriging.F90:660-661, after
+     * the simulation branch) */
+    k2 = 0;
+    for (int i = 0; i < no; ++i)
+      if (dob[i] <= maxd2) io[k2++] = io[i];
+    no = k2;
     isort(io, no);
     if (R->nnear) { R->nnear[(size_t)node * 2] = no; R->nnear[(size_t)node * 2 + 1] = nbk; }
     if (R->inear) {
@@ -1924,7 +1975,7 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
     }
   }
   free(f.L); free(f.Y); free(f.S); free(f.Afac); free(f.ipiv);
-  free(A); free(B); free(X); free(work); free(h); free(io); free(ib_); free(db); free(vals);
+  free(A); free(B); free(X); free(work); free(h); free(dob); free(io); free(ib_); free(db); free(vals);
   kd_free(&tree);
   free(xc); free(sc);
   model_free(&c->mdl[0][0]);

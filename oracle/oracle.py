@@ -346,7 +346,10 @@ class OracleKriging:
         P, keep = self._problem(nthread=1, ncache=0)
         nb = P.nblock
         nmax = int(self.obs[0]["nmax"])
-        mm = min(max(nmax, 1), self.obs[0]["coord"].shape[0] + nb)
+        ntot = self.obs[0]["coord"].shape[0] + nb
+        if nmax <= 0 or nmax > ntot:
+            nmax = ntot
+        mm = min((2 ** self.ndim) * nmax if P.sector[0] else nmax, ntot)
         self.value = np.full((nb, self.nsim), np.nan)
         self.variance = np.full(nb, np.nan)
         self.sim_nnear = np.zeros((nb, 2), dtype=np.int32)

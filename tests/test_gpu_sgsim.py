@@ -182,3 +182,39 @@ def test_sgsim_lattice_at_table_zone_edges():
     vgm = w1["vgm"][0][2]
     g, o = _pair(ob["coord"], ob["value"], grid, vgm, 2, path, sample, nmax=24)
     _check(g, o, float(np.ptp(ob["value"])), 2)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_sgsim_sector_search(ndim):
+    """Sector search in the simulation (kriging.F90:533-553): the sorted
+    candidates among the observations and earlier targets through the
+    sector filter, with maxdist on observations and targets."""
+    rng = np.random.default_rng(30 + ndim)
+    nobs, nt = (400, 1600) if ndim == 2 else (500, 1200)
+    obs = rng.uniform(0, 10, (nobs, ndim))
+    z = np.sin(obs[:, 0]) + np.cos(0.7 * obs[:, 1]) + (0.3 * obs[:, 2] if ndim == 3 else 0.0)
+    grid = rng.uniform(0, 10, (nt, ndim))
+    path = rng.permutation(nt) + 1
+    sample = rng.normal(0, 1, nt)
+    vgm = dict(vtype="sph", nugget=0.02, sill=1.0, a_major=4.0, a_minor1=2.0, azimuth=35.0)
+    search = dict(anis1=0.5, azimuth=35.0, sector_search=True)
+    g, o = _pair(obs, z, grid, vgm, 1, path, sample, nmax=6, search=search, obs_kw=dict(maxdist=3.5),
+                 anisotropic_search=True)
+    _check(g, o, float(np.ptp(z)), 1)
+    assert o.sim_nnear[:, 1].max() > 0 and o.sim_nnear.sum(axis=1).max() <= (2 ** ndim) * 6
+
+
+def test_sgsim_maxdist_on_observations():
+    """maxdist cuts observation members as well as simulated ones
+    (kriging.F90:660-661), in the kd-tree branch and in the branch where
+    every observation and earlier target fits within nmax."""
+    rng = np.random.default_rng(12)
+    obs = rng.uniform(0, 10, (60, 2))
+    z = np.cos(obs[:, 0]) * np.sin(0.5 * obs[:, 1])
+    grid = rng.uniform(0, 10, (500, 2))
+    path = rng.permutation(len(grid)) + 1
+    sample = rng.normal(0, 1, len(grid))
+    vgm = dict(vtype="exp", nugget=0.05, sill=1.0, a_major=3.0)
+    g, o = _pair(obs, z, grid, vgm, 1, path, sample, nmax=70, obs_kw=dict(maxdist=2.5))
+    _check(g, o, float(np.ptp(z)), 1)
+    assert (o.sim_nnear[:, 0] < 60).all() and o.sim_nnear[:, 0].min() > 0

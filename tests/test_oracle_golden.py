@@ -272,3 +272,60 @@ def test_sgsim_grid_on_observations():
     est, _ = o.solve().get_results()
     assert np.isnan(est).sum() == 0
     np.testing.assert_allclose(est, value, rtol=1e-2, atol=1e-2)
+
+
+def _first_target_vs_kriging(search, obs_kw, nmax=12):
+    """SGSIM's first visited target sees only the observations: with a zero
+    draw its value and variance equal ordinary kriging under the same search
+    (sectors, maxdist)."""
+    rng = np.random.default_rng(21)
+    obs = rng.uniform(0, 10, (150, 2))
+    z = np.sin(obs[:, 0]) + 0.5 * np.cos(obs[:, 1])
+    grid = rng.uniform(0, 10, (60, 2))
+    path = rng.permutation(len(grid)) + 1
+    vgm = dict(vtype="exp", nugget=0.05, sill=1.0, a_major=3.0, a_minor1=1.5, azimuth=20.0)
+    o = OracleKriging(ndim=2, nvar=1, nsim=1, anisotropic_search=True)
+    o.set_obs(1, obs, z, nmax=nmax, **obs_kw)
+    o.set_vgm(1, 1, **vgm)
+    o.set_grid(grid)
+    o.set_search(1, **search)
+    o.set_sim(path, np.zeros(len(grid)))
+    sims, var = o.solve().get_results()
+    first = path[0] - 1
+    k = OracleKriging(ndim=2, nvar=1, anisotropic_search=True)
+    k.set_obs(1, obs, z, nmax=nmax, **obs_kw)
+    k.set_vgm(1, 1, **vgm)
+    k.set_grid(grid[first:first + 1])
+    k.set_search(1, **search)
+    e, v = k.solve().get_results()
+    assert o.sim_nnear[first, 1] == 0
+    assert o.sim_nnear[first, 0] == k.nnear[0, 0]
+    np.testing.assert_array_equal(o.sim_inear[first, :k.nnear[0, 0]], k.neighbours(0) - 1)
+    assert abs(sims[first] - e[0]) <= 1e-12 * max(1.0, abs(e[0]))
+    assert abs(var[first] - v[0]) <= 1e-12
+    return o, obs, grid
+
+
+def test_sgsim_sector_search_first_target_and_sector_caps():
+    """Sector search in the simulation (kriging.F90:533-553): the first
+    target's set is the kriging sector set; every later set holds at most
+    four sectors of nmax members, observations and earlier targets together."""
+    o, obs, grid = _first_target_vs_kriging(dict(anis1=0.5, azimuth=20.0, sector_search=True), {}, nmax=5)
+    path = o.sim_path
+    pos = np.empty(len(grid), dtype=int)
+    pos[path - 1] = np.arange(len(grid))
+    for t in range(len(grid)):
+        n = int(o.sim_nnear[t].sum())
+        idx = o.sim_inear[t, :n]
+        assert n <= 4 * 5
+        assert (idx[o.sim_nnear[t, 0]:] >= len(obs)).all() and (idx[:o.sim_nnear[t, 0]] < len(obs)).all()
+        assert (idx[o.sim_nnear[t, 0]:] - len(obs) < pos[t]).all()  # only targets visited before
+    assert o.sim_nnear[:, 1].max() > 0
+
+
+def test_sgsim_maxdist_applies_to_observations():
+    """maxdist cuts the observation members too (filter_by_maxlag after the
+    simulation branch, kriging.F90:660-661): the first target equals
+    kriging with the same maxdist, and no member lies beyond it."""
+    o, obs, grid = _first_target_vs_kriging(dict(anis1=0.5, azimuth=20.0), dict(maxdist=1.5), nmax=16)
+    assert (o.sim_nnear[:, 0] < 16).any()
