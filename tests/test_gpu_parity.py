@@ -206,3 +206,22 @@ def test_ties_use_exact_kdtree_order():
         g, o = _run_pair(w, "fp64")
         _check_neighbours(g, o)
         _check_values(g, o, w, 1e-9)
+
+
+@pytest.mark.parametrize("sector", [False, True])
+def test_ties_lattice_grid(sector):
+    """A 60 x 60 lattice of observations and 7 081 targets on the lattice
+    points and the cell centres: every target has equal distances at its
+    selection boundary, so most of them go through the kd-tree replica."""
+    xs, ys = np.meshgrid(np.arange(60.0), np.arange(60.0))
+    obs = np.column_stack([xs.ravel(), ys.ravel()])
+    z = np.sin(0.3 * obs[:, 0]) + np.cos(0.2 * obs[:, 1])
+    cx, cy = np.meshgrid(np.arange(59.0) + 0.5, np.arange(59.0) + 0.5)
+    tg = np.vstack([obs, np.column_stack([cx.ravel(), cy.ravel()])])
+    w = dict(ndim=2, nvar=1, kw={}, obs=[dict(coord=obs, value=z, nmax=7 if not sector else 3)],
+             vgm=[(1, 1, dict(vtype="exp", nugget=0.1, sill=1.0, a_major=6.0))],
+             search=[dict(sector_search=sector)], grid=tg, zstd=float(np.std(z)), sill=1.1)
+    g, o = _run_pair(w, "fp64")
+    _check_neighbours(g, o)
+    _check_values(g, o, w, 1e-9)
+    assert g.gpu_counters()["search_redo"][0] > len(tg) // 4
