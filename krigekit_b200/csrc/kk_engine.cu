@@ -1346,7 +1346,6 @@ static void engine_sgsim(Engine& e) {
                       "GPU library; simulate one variable");
   if (e.st) throw std::string("space-time sequential simulation is not supported by the GPU library");
   if (!e.nblockpnt.empty()) throw std::string("sequential simulation needs point targets (set_grid)");
-  if (e.ndrift > 0) throw std::string("sequential simulation with external drift is not supported by the GPU library");
   if (e.store_weight || e.use_old_weight) throw std::string("the weight store is not used with sequential simulation");
   if (e.obs.empty() || e.obs[0].n == 0) throw std::string("Observations need to be set first.");
   if (e.nblock == 0) throw std::string("Grid needs to be set first.");
@@ -1381,7 +1380,7 @@ static void engine_sgsim(Engine& e) {
   s.ndim = e.ndim;
   s.nlag = e.nlag;
   s.nvar = 1;
-  s.ndrift = 0;
+  s.ndrift = e.ndrift;
   s.unbias = e.unbias;
   s.anisotropic_search = e.anisotropic_search;
   s.neglect_error = e.neglect_error;
@@ -1402,6 +1401,20 @@ static void engine_sgsim(Engine& e) {
     for (int k = 0; k < D; ++k) so.coord[(size_t)(nobs + p) * D + k] = bc[(size_t)(e.sim_path[p] - 1) * D + k];
   so.value.resize(so.n, 0.0);
   so.variance.resize(so.n, 0.0);  // simulated targets carry no measurement error
+  const int nd = e.ndrift;
+  if (nd > 0) {
+    // a simulated member's drift row is the target drift at its node
+    // (block%drift in visiting order, kriging.F90:789-794)
+    if (e.bdrift.size() != (size_t)nd * nb) throw std::string("Grid drift is not set while ndrift > 0.");
+    so.drift.resize((size_t)nd * so.n);
+    s.bdrift.resize((size_t)nd * nb);
+    for (int p = 0; p < nb; ++p)
+      for (int a = 0; a < nd; ++a) {
+        const double g = e.bdrift[(size_t)(e.sim_path[p] - 1) * nd + a];
+        so.drift[(size_t)(nobs + p) * nd + a] = g;
+        s.bdrift[(size_t)p * nd + a] = g;
+      }
+  }
   so.dirty = true;
   so.search_dirty = true;
   s.vgm[0][0] = e.vgm[0][0];

@@ -1720,9 +1720,9 @@ done:
 int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int nsim, orc_sim_result *R) {
   R->err = 0;
   R->errmsg[0] = 0;
-  if (P->nvar != 1 || P->st || P->nblockpnt || P->ndrift > 0 || P->cross_validation) {
+  if (P->nvar != 1 || P->st || P->nblockpnt || P->cross_validation) {
     R->err = 1;
-    snprintf(R->errmsg, 256, "sgsim: one variable, point targets, no drift or cross-validation");
+    snprintf(R->errmsg, 256, "sgsim: one variable, point targets, no cross-validation");
     return 1;
   }
   const int nb = P->nblock, nobs = P->nobs[0], ndim = P->ndim, nlag = ndim;
@@ -1748,8 +1748,8 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
   c->ndim = ndim;
   c->nlag = nlag;
   c->naug = P->unbias;
-  c->pa = c->naug;
-  const int pa = c->pa;
+  c->pa = P->ndrift + c->naug;
+  const int pa = c->pa, ndr = P->ndrift;
   if (P->nstruct[0][0] == 0) {
     R->err = 1;
     snprintf(R->errmsg, 256, "variogram not set for ivar=1, jvar=1");
@@ -1912,7 +1912,16 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
         lag_of(c, SG_X(i), SG_X(j), rs, lag);
         A[j + (size_t)i * m] = pair_cov(c, 0, 0, lag);
       }
-      for (int r = 0; r < pa; ++r) A[(npp + r) + (size_t)i * m] = 1.0;
+      /* drift rows, then unbiasedness (kriging.F90:789-794): the observation
+       * drift for observation members, the target drift at the simulated
+       * target's node for simulated members (block%drift in visiting order) */
+      for (int r = 0; r < pa; ++r) {
+        double fv = 1.0;
+        if (r < ndr)
+          fv = i < no ? P->obs_drift[0][(size_t)io[i] * ndr + r]
+                      : P->block_drift[(size_t)(path[ib_[i - no]] - 1) * ndr + r];
+        A[(npp + r) + (size_t)i * m] = fv;
+      }
     }
     for (int ir = 0; ir < npp; ++ir)
       for (int ic = ir + 1; ic < m; ++ic) A[ir + (size_t)ic * m] = A[ic + (size_t)ir * m];
@@ -1921,7 +1930,7 @@ int orc_sgsim(const orc_problem *P, const int *path, const double *sample, int n
       lag_of(c, SG_X(k), xloc, rs, lag);
       B[k] = pair_cov(c, 0, 0, lag);
     }
-    for (int r = 0; r < pa; ++r) B[npp + r] = 1.0;
+    for (int r = 0; r < pa; ++r) B[npp + r] = r < ndr ? P->block_drift[(size_t)node * ndr + r] : 1.0;
 #undef SG_X
     int info = chol_setup(npp, pa, A, m, &f);
     if (info == 0) {

@@ -218,3 +218,29 @@ def test_sgsim_maxdist_on_observations():
     g, o = _pair(obs, z, grid, vgm, 1, path, sample, nmax=70, obs_kw=dict(maxdist=2.5))
     _check(g, o, float(np.ptp(z)), 1)
     assert (o.sim_nnear[:, 0] < 60).all() and o.sim_nnear[:, 0].min() > 0
+
+
+def test_sgsim_external_drift():
+    """Kriging with two external drifts in the simulation: the simulated
+    members carry the target drift at their nodes."""
+    rng = np.random.default_rng(43)
+    obs = rng.uniform(0, 10, (500, 2))
+    grid = rng.uniform(0, 10, (2000, 2))
+    dfun = lambda x: np.column_stack([np.sin(0.4 * x[:, 0]), 0.1 * x[:, 1]])
+    z = 0.8 * dfun(obs)[:, 0] - 0.5 * dfun(obs)[:, 1] + 0.2 * np.cos(obs[:, 1])
+    path = rng.permutation(len(grid)) + 1
+    sample = rng.normal(0, 1, (len(grid), 2))
+    from krigekit_b200 import Kriging
+    g = Kriging(ndim=2, nvar=1, ndrift=2, nsim=2, seed=3)
+    o = OracleKriging(ndim=2, nvar=1, ndrift=2, nsim=2)
+    for k in (g, o):
+        k.set_obs(1, obs, z, nmax=20)
+        k.set_obs_drift(1, dfun(obs))
+        k.set_vgm(1, 1, vtype="sph", nugget=0.02, sill=0.5, a_major=4.0)
+        k.set_grid(grid)
+        k.set_grid_drift(dfun(grid))
+        k.set_search(1)
+        k.set_sim(path, sample)
+    g.solve()
+    o.solve()
+    _check(g, o, float(np.ptp(z)), 2)

@@ -329,3 +329,35 @@ def test_sgsim_maxdist_applies_to_observations():
     kriging with the same maxdist, and no member lies beyond it."""
     o, obs, grid = _first_target_vs_kriging(dict(anis1=0.5, azimuth=20.0), dict(maxdist=1.5), nmax=16)
     assert (o.sim_nnear[:, 0] < 16).any()
+
+
+def test_sgsim_external_drift_first_target_is_ked():
+    """External drift in the simulation (kriging.F90:789-794, 936-937): the
+    first visited target is kriging with external drift; later systems carry
+    the target drift of their simulated members."""
+    rng = np.random.default_rng(41)
+    obs = rng.uniform(0, 10, (200, 2))
+    grid = rng.uniform(0, 10, (120, 2))
+    dfun = lambda x: np.column_stack([np.sin(0.4 * x[:, 0]), 0.1 * x[:, 1]])
+    z = 0.8 * dfun(obs)[:, 0] - 0.5 * dfun(obs)[:, 1] + 0.2 * np.cos(obs[:, 1])
+    path = rng.permutation(len(grid)) + 1
+    vgm = dict(vtype="sph", nugget=0.02, sill=0.5, a_major=4.0)
+
+    def setup(k, g):
+        k.set_obs(1, obs, z, nmax=14)
+        k.set_obs_drift(1, dfun(obs))
+        k.set_vgm(1, 1, **vgm)
+        k.set_grid(g)
+        k.set_grid_drift(dfun(g))
+        k.set_search(1)
+        return k
+
+    o = setup(OracleKriging(ndim=2, nvar=1, ndrift=2, nsim=1), grid)
+    o.set_sim(path, np.zeros(len(grid)))
+    sims, var = o.solve().get_results()
+    first = path[0] - 1
+    k = setup(OracleKriging(ndim=2, nvar=1, ndrift=2), grid[first:first + 1])
+    e, v = k.solve().get_results()
+    assert abs(sims[first] - e[0]) <= 1e-12 * max(1.0, abs(e[0]))
+    assert abs(var[first] - v[0]) <= 1e-12
+    assert np.isfinite(sims).all() and o.sim_nnear[:, 1].max() > 0
