@@ -244,3 +244,29 @@ def test_sgsim_external_drift():
     g.solve()
     o.solve()
     _check(g, o, float(np.ptp(z)), 2)
+
+
+def test_sgsim_3d_rangescale_and_local_nugget():
+    """3-D simulation with a per-target range scale and local nugget (the
+    lags of a target's system scaled by its range scale, its nugget on the
+    diagonal of observation and simulated members alike)."""
+    from krigekit_b200 import Kriging
+    rng = np.random.default_rng(51)
+    obs = rng.uniform(0, 5, (400, 3))
+    z = np.sin(obs[:, 0]) + np.cos(obs[:, 1]) * 0.5 + 0.2 * obs[:, 2]
+    grid = rng.uniform(0, 5, (1500, 3))
+    path = rng.permutation(len(grid)) + 1
+    sample = rng.normal(0, 1, len(grid))
+    rs = rng.uniform(0.7, 1.4, len(grid))
+    ln = rng.uniform(0.0, 0.05, len(grid))
+    g = Kriging(ndim=3, nvar=1, nsim=1, seed=2)
+    o = OracleKriging(ndim=3, nvar=1, nsim=1)
+    for k in (g, o):
+        k.set_obs(1, obs, z, nmax=18)
+        k.set_vgm(1, 1, vtype="exp", nugget=0.05, sill=1.0, a_major=2.0, a_minor1=1.5, a_minor2=1.0, azimuth=15.0)
+        k.set_grid(grid, rangescale=rs, localnugget=ln)
+        k.set_search(1)
+        k.set_sim(path, sample)
+    g.solve()
+    o.solve()
+    _check(g, o, float(np.ptp(z)), 1)
