@@ -14,7 +14,6 @@
 #include <memory>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "kk_host.h"
@@ -53,30 +52,6 @@ static Engine* get(int64_t h) {
 }
 
 static int ierr() { return failed() ? 1 : 0; }
-
-// Host memcpy of a large array split over threads: a caller's freshly
-// allocated output pages are first touched here, and one core faults them in
-// at a few GB/s.
-static void par_copy(void* dst, const void* src, size_t bytes) {
-  constexpr size_t kPiece = size_t(4) << 20;
-  const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nt = std::min<size_t>({size_t(8), size_t(hc), bytes / kPiece});
-  if (nt <= 1) {
-    if (bytes) std::memcpy(dst, src, bytes);
-    return;
-  }
-  const size_t per = ((bytes + nt - 1) / nt + 63) & ~size_t(63);
-  std::vector<std::thread> th;
-  th.reserve(nt - 1);
-  for (size_t i = 1; i < nt; ++i) {
-    const size_t lo = i * per;
-    if (lo >= bytes) break;
-    const size_t n = std::min(per, bytes - lo);
-    th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, n); });
-  }
-  std::memcpy(dst, src, std::min(per, bytes));
-  for (auto& t : th) t.join();
-}
 
 // device -> host copy of solve results, with the CUDA status checked
 static void copy_d2h(void* dst, const void* src, size_t bytes) {
@@ -279,14 +254,14 @@ int krige_set_obs(int64_t h, int ivar, int nobs, int ndim_c, const double* coord
   if (variance) o.variance.assign(variance, variance + nobs);
   else o.variance.assign(nobs, 0.0);
   // duplicate coordinate check (check_duplicate_coordinates_base, utils.F90:43-133):
-  // open-addressing hash table over all coordinates, full comparison on a
-  // matching slot (equal coordinates always hash alike)
+  // open-addressing hash tables over all coordinates, full comparison on a
+  // matching slot (equal coordinates always hash alike).  The hash's top
+  // bits split the points into partitions, one table and thread each; every
+  // partition scans in index order, so the reported pair (the smallest index
+  // that repeats an earlier point, and that point) is the sequential scan's.
   {
     const double* c = o.coord.data();
-    size_t cap = 1;
-    while (cap < 2 * (size_t)nobs + 2) cap <<= 1;
-    std::vector<int> slot(cap, -1);
-    for (int i = 0; i < nobs; ++i) {
+    auto hash_of = [=](int i) {
       uint64_t hsh = 0x9e3779b97f4a7c15ull;
       for (int k = 0; k < ndim_c; ++k) {
         double v = c[(size_t)i * ndim_c + k];
@@ -297,21 +272,55 @@ int krige_set_obs(int64_t h, int ivar, int nobs, int ndim_c, const double* coord
         hsh *= 0xff51afd7ed558ccdull;
         hsh ^= hsh >> 33;
       }
-      size_t p = hsh & (cap - 1);
-      while (slot[p] >= 0) {
-        const int j = slot[p];
-        bool same = true;
-        for (int k = 0; k < ndim_c; ++k)
-          if (c[(size_t)i * ndim_c + k] != c[(size_t)j * ndim_c + k]) { same = false; break; }
-        if (same) {
-          char msg[160];
-          snprintf(msg, sizeof msg, "Duplicate observation coordinates at points %d and %d", j + 1, i + 1);
-          o = ObsVar();
-          throw std::string(msg);
+      return hsh;
+    };
+    const int nparts = nobs >= (1 << 16) ? 8 : 1;
+    std::vector<int> dup_i(nparts, INT_MAX), dup_j(nparts, -1);
+    par_for((size_t)nparts, 1, [&](size_t p0, size_t p1) {
+      for (size_t part = p0; part < p1; ++part) {
+        size_t cap = 1;
+        while (cap < 2 * ((size_t)nobs / nparts + 1) + 2) cap <<= 1;
+        std::vector<int> slot(cap, -1);
+        size_t used = 0;
+        for (int i = 0; i < nobs; ++i) {
+          const uint64_t hsh = hash_of(i);
+          if (nparts > 1 && (size_t)(hsh >> 61) != part) continue;
+          if (2 * (used + 1) > cap) {  // a skewed partition: grow and reinsert
+            std::vector<int> old;
+            old.swap(slot);
+            cap <<= 1;
+            slot.assign(cap, -1);
+            for (int j : old) {
+              if (j < 0) continue;
+              size_t q = hash_of(j) & (cap - 1);
+              while (slot[q] >= 0) q = (q + 1) & (cap - 1);
+              slot[q] = j;
+            }
+          }
+          size_t q = hsh & (cap - 1);
+          bool found = false;
+          while (slot[q] >= 0) {
+            const int j = slot[q];
+            bool same = true;
+            for (int k = 0; k < ndim_c; ++k)
+              if (c[(size_t)i * ndim_c + k] != c[(size_t)j * ndim_c + k]) { same = false; break; }
+            if (same) { dup_i[part] = i; dup_j[part] = j; found = true; break; }
+            q = (q + 1) & (cap - 1);
+          }
+          if (found) break;
+          slot[q] = i;
+          ++used;
         }
-        p = (p + 1) & (cap - 1);
       }
-      slot[p] = i;
+    });
+    int bi = INT_MAX, bj = -1;
+    for (int part = 0; part < nparts; ++part)
+      if (dup_i[part] < bi) { bi = dup_i[part]; bj = dup_j[part]; }
+    if (bj >= 0) {
+      char msg[160];
+      snprintf(msg, sizeof msg, "Duplicate observation coordinates at points %d and %d", bj + 1, bi + 1);
+      o = ObsVar();
+      throw std::string(msg);
     }
   }
   o.nmax = nmax;
@@ -560,7 +569,7 @@ int krige_set_grid_drift(int64_t h, int ivar, int ndrift_c, int nblocks, const d
   if (ivar == 0 || ivar > e->nvar) throw std::string("ivar must be 1..nvar or < 0 (broadcast)");
   if (e->nvar == 1) {
     // (ndrift, nblock) is already the (ndrift, nvar, nblock) layout
-    std::memcpy(e->bdrift.data(), drift, sizeof(double) * (size_t)nblocks * ndrift_c);
+    par_copy(e->bdrift.data(), drift, sizeof(double) * (size_t)nblocks * ndrift_c);
   } else {
     for (int ib = 0; ib < nblocks; ++ib)
       for (int v = 0; v < e->nvar; ++v) {
@@ -678,8 +687,10 @@ int krige_get_estimate_all(int64_t h, int nblocks, int nvar_c, int nsim_c, doubl
   } else {
     std::vector<double> fb;
     const double* tmp = results_to_host(e, e->est.p, (size_t)e->nblock * nv, fb);
-    for (int iv = 0; iv < nvar_c; ++iv)
-      for (int ib = 0; ib < nblocks; ++ib) out[ib + (size_t)nblocks * iv] = tmp[(size_t)ib * nv + iv];
+    par_for((size_t)nblocks, size_t(1) << 18, [=](size_t lo, size_t hi) {
+      for (int iv = 0; iv < nvar_c; ++iv)
+        for (size_t ib = lo; ib < hi; ++ib) out[ib + (size_t)nblocks * iv] = tmp[ib * nv + iv];
+    });
   }
   // every realisation slot holds the kriging estimate (no simulation)
   for (int is = 1; is < nsim_c; ++is)
@@ -764,10 +775,12 @@ int krige_get_variance_all(int64_t h, int nblocks, int nvar_c, double* out) {
   } else {
     std::vector<double> fb;
     const double* tmp = results_to_host(e, e->var.p, (size_t)e->nblock * nv * nv, fb);
-    for (int jv = 0; jv < nvar_c; ++jv)
-      for (int iv = 0; iv < nvar_c; ++iv)
-        for (int ib = 0; ib < nblocks; ++ib)
-          out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * jv)] = tmp[(size_t)ib * nv * nv + iv + (size_t)jv * nv];
+    par_for((size_t)nblocks, size_t(1) << 18, [=](size_t lo, size_t hi) {
+      for (int jv = 0; jv < nvar_c; ++jv)
+        for (int iv = 0; iv < nvar_c; ++iv)
+          for (size_t ib = lo; ib < hi; ++ib)
+            out[ib + (size_t)nblocks * (iv + (size_t)nvar_c * jv)] = tmp[ib * nv * nv + iv + (size_t)jv * nv];
+    });
   }
   KK_GUARD_END
 }
@@ -1189,10 +1202,13 @@ int krige_st_set_vgm_joint_sills(int64_t h, int ivar, int jvar, int nsill, const
 static void st_coords(const Engine* e, int n, const double* coord, const double* time, std::vector<double>& c) {
   const int nd = e->ndim;
   c.resize((size_t)(nd + 1) * n);
-  for (int i = 0; i < n; ++i) {
-    for (int k = 0; k < nd; ++k) c[(size_t)i * (nd + 1) + k] = coord[(size_t)i * nd + k];
-    c[(size_t)i * (nd + 1) + nd] = time[i];
-  }
+  double* cp = c.data();
+  par_for((size_t)n, size_t(1) << 18, [=](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) {
+      for (int k = 0; k < nd; ++k) cp[i * (nd + 1) + k] = coord[i * nd + k];
+      cp[i * (nd + 1) + nd] = time[i];
+    }
+  });
 }
 
 // krige_st_set_grid, kriging_st_capi.f90:331-353: coord(ndim, ngrid), time(ngrid)
@@ -1230,9 +1246,11 @@ int krige_st_set_grid_block(int64_t h, int nblocks, const double* coord, const d
   if (tot != npnts_total) throw std::string("sum(nblockpnt) /= size(blockcoord, 2)");
   st_coords(e, nblocks, coord, time, e->bcoord);
   e->bcoord_staged = false;
-  e->nblockpnt.assign(nblockpnt, nblockpnt + nblocks);
+  e->nblockpnt.resize(nblocks);
+  par_copy(e->nblockpnt.data(), nblockpnt, sizeof(int) * (size_t)nblocks);
   st_coords(e, npnts_total, blockcoord, blocktime, e->gcoord);
-  e->gweight.assign(pointweight, pointweight + npnts_total);
+  e->gweight.resize(npnts_total);
+  par_copy(e->gweight.data(), pointweight, sizeof(double) * (size_t)npnts_total);
   grid_common(e, nblocks, rangescale, localnugget);
   KK_GUARD_END
 }

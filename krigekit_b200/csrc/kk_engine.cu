@@ -629,8 +629,11 @@ void engine_solve(Engine& e) {
         e.launches += 1;
       }
     } else {
-      for (int i = 0; i < nb; ++i)
-        for (int k = 0; k < D; ++k) hs[(size_t)k * nb + i] = e.bcoord[(size_t)i * D + k];
+      const double* bc = e.bcoord.data();
+      par_for((size_t)nb, size_t(1) << 18, [=](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i)
+          for (int k = 0; k < D; ++k) hs[(size_t)k * nb + i] = bc[i * D + k];
+      });
       for (int k = 0; k < D; ++k) upload(e.tx[k], hs + (size_t)k * nb, sizeof(double) * nb, st);
     }
     for (int k = D; k < 4; ++k) e.tx[k].reserve(8);
@@ -638,9 +641,12 @@ void engine_solve(Engine& e) {
     if (!e.localnugget.empty()) upload(e.tln, e.localnugget.data(), sizeof(double) * nb, st);
     if (blocks) {
       double* hn = hs + (size_t)nb * D;  // nodes per axis, then the weights
-      for (size_t i = 0; i < ng; ++i)
-        for (int k = 0; k < D; ++k) hn[(size_t)k * ng + i] = e.gcoord[i * D + k];
-      std::memcpy(hn + (size_t)D * ng, e.gweight.data(), sizeof(double) * ng);
+      const double* gc = e.gcoord.data();
+      par_for(ng, size_t(1) << 18, [=](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i)
+          for (int k = 0; k < D; ++k) hn[(size_t)k * ng + i] = gc[i * D + k];
+      });
+      par_copy(hn + (size_t)D * ng, e.gweight.data(), sizeof(double) * ng);
       int* gs = reinterpret_cast<int*>(hn + (size_t)(D + 1) * ng);
       gs[0] = 0;
       for (int i = 0; i < nb; ++i) gs[i + 1] = gs[i] + e.nblockpnt[i];

@@ -2,9 +2,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cfloat>
+#include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kk_common.h"
@@ -12,6 +15,36 @@
 #define KK_CNT_N_HOST 32  // = KK_CNT_N (kk_kernels.h)
 
 namespace kk {
+
+// f(lo, hi) over [0, n) in up to eight host threads, pieces of at least
+// `grain` items (inline below that): the host-side copies and transposes of
+// millions of targets and nodes run at memory rather than single-core speed.
+template <class F>
+inline void par_for(size_t n, size_t grain, F f) {
+  const size_t hc = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({size_t(8), hc, grain ? n / grain : size_t(1)});
+  if (nt <= 1) {
+    if (n) f(size_t(0), n);
+    return;
+  }
+  const size_t per = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (size_t i = 1; i < nt; ++i) {
+    const size_t lo = i * per, hi = std::min(n, lo + per);
+    if (lo < hi) th.emplace_back([=] { f(lo, hi); });
+  }
+  f(size_t(0), std::min(n, per));
+  for (auto& t : th) t.join();
+}
+
+// memcpy of a large array over threads (a caller's freshly allocated pages
+// are first touched here, which one core does at a few GB/s)
+inline void par_copy(void* dst, const void* src, size_t bytes) {
+  par_for(bytes, size_t(4) << 20, [=](size_t lo, size_t hi) {
+    std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
+  });
+}
 
 struct StructSpec {
   int vtype = KK_SPH;

@@ -204,3 +204,24 @@ def test_duplicate_observations_raise():
     with pytest.raises(RuntimeError):
         k.set_obs(1, x, np.array([1.0, 2.0, 3.0]))
     k.close()
+
+
+def test_duplicate_observations_large_set_reports_first_pair():
+    """The duplicate check of a large observation set (hash partitions over
+    threads) reports the pair the reference's sequential scan finds first:
+    the smallest index that repeats an earlier point, and that point."""
+    from krigekit_b200 import Kriging
+    rng = np.random.default_rng(8)
+    x = rng.uniform(0, 1, (100_000, 2))
+    x[90_000] = x[5]
+    x[70_000] = x[12_345]
+    x[80_000] = -0.0 * x[80_000] + x[3]  # equal coordinates again, later index
+    k = Kriging(ndim=2, nvar=1)
+    with pytest.raises(RuntimeError, match="points 12346 and 70001"):
+        k.set_obs(1, x, np.zeros(len(x)))
+    x[70_000] += 1e-9
+    with pytest.raises(RuntimeError, match="points 4 and 80001"):
+        k.set_obs(1, x, np.zeros(len(x)))
+    x[[80_000, 90_000]] += 1e-9
+    k.set_obs(1, x, np.zeros(len(x)))  # no duplicates left
+    k.close()
