@@ -216,7 +216,8 @@ int krige_gpu_stats(int64_t handle, int *out8, double *solve_ms);
  * list, [4] FP32 systems re-solved in FP64, [5] failures (NaN), [6] Cholesky solves,
  * [7] LDL^T solves, [16..19] search fallbacks per variable, [20] refinement passes,
  * [21] LDL^T solves that needed the 1e-6 mean-diagonal jitter, [22] targets with
- * 65..128 neighbours. */
+ * 65..128 neighbours; after a simulation (nsim > 0) [24] 1 when its draws ran as one
+ * launch (0: level by level) and [25] its number of dependency levels. */
 int krige_gpu_counters(int64_t handle, int n, int *out);
 /* No counterpart in the reference (its solver has one CPU path).  How krige_solve picks
  * the kernel for each neighbour-count list (2..32, 33..64, > 128, 65..128 equations):

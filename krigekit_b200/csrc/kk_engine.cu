@@ -1506,10 +1506,31 @@ static void engine_sgsim(Engine& e) {
   SP.hi = e.bounds[1];
   PhaseTimer timer(e);
   timer.start();
-  for (int L = 0; L < nlev; ++L) {
-    launch_sgsim_level(SP, dorder.as<int>() + off[L], off[L + 1] - off[L], nsm, st);
+  // every level in one launch; level by level when the device cannot take a
+  // cooperative launch or a wait ran past its limit
+  DBuf dflags;
+  dflags.reserve(sizeof(int) * ((size_t)nb + 2));
+  KK_CUDA(cudaMemsetAsync(dflags.p, 0, sizeof(int) * ((size_t)nb + 2), st));
+  int* flags = dflags.as<int>();
+  bool flow = launch_sgsim_flow(SP, dorder.as<int>(), nb, flags, flags + nb, flags + nb + 1, nsm, st);
+  int nlaunch = 1;
+  if (flow) {
     KK_CUDA(cudaGetLastError());
+    int ferr = 0;
+    KK_CUDA(cudaMemcpyAsync(&ferr, flags + nb + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KK_CUDA(cudaStreamSynchronize(st));
+    flow = ferr == 0;
+  } else {
+    cudaGetLastError();
   }
+  if (!flow) {
+    for (int L = 0; L < nlev; ++L) {
+      launch_sgsim_level(SP, dorder.as<int>() + off[L], off[L + 1] - off[L], nsm, st);
+      KK_CUDA(cudaGetLastError());
+    }
+    nlaunch += nlev;
+  }
+  e.sim_flow = flow ? 1 : 0;
   timer.stop(2);
 
   // ---- variance and status in target order
@@ -1528,9 +1549,11 @@ static void engine_sgsim(Engine& e) {
   for (int i = 0; i < 4; ++i) e.phase_ms[i] += s.phase_ms[i];
   e.phase_ms[4] = s.phase_ms[4];
   e.phase_ms[5] = s.phase_ms[5];
-  e.launches += s.launches + nlev;
+  e.launches += s.launches + nlaunch;
   std::memcpy(e.stats, s.stats, sizeof e.stats);
   std::memcpy(e.counters_last, s.counters_last, sizeof e.counters_last);
+  e.counters_last[24] = e.sim_flow;  // host-side slots of krige_gpu_counters
+  e.counters_last[25] = nlev;
   for (int li = 0; li < KK_NLIST; ++li) {
     e.plan[li] = s.plan[li];
     for (int k = 0; k < KK_NKER; ++k) e.plan_us[li][k] = s.plan_us[li][k];

@@ -131,6 +131,11 @@ struct SimParams {
   double sk_mean, lo, hi;
 };
 void launch_sgsim_level(const SimParams& S, const int* list, int count, int nsm, cudaStream_t st);
+// All levels in one cooperative launch (positions in level order; done, work
+// and err zeroed); false when the device cannot take it.  *err turns 1 when a
+// wait for a neighbour ran past its limit (the values are then NaN).
+bool launch_sgsim_flow(const SimParams& S, const int* order, int count, int* done, int* work, int* err, int nsm,
+                       cudaStream_t st);
 
 void launch_bucket(const SolveParams& P, int* lists, cudaStream_t st);
 // Estimates of every target from the weight store (P.wout, P.nbr, P.nnear)

@@ -367,7 +367,8 @@ class Kriging:
         return {"bucket_le32": buf[0], "bucket_le64": buf[1], "bucket_gt128": buf[2], "bucket_le128": buf[22],
                 "general_list": buf[3],
                 "fp64_resolve": buf[4], "fail": buf[5], "chol": buf[6], "ldlt": buf[7],
-                "search_redo": [buf[16 + v] for v in range(4)], "refine_passes": buf[20], "jitter": buf[21]}
+                "search_redo": [buf[16 + v] for v in range(4)], "refine_passes": buf[20], "jitter": buf[21],
+                "sim_one_launch": buf[24], "sim_levels": buf[25]}
 
     def set_autotune(self, mode: int = 1):
         """Kernel choice per neighbour-count list (extension; krige_set_autotune):

@@ -72,6 +72,8 @@ def test_sgsim_reference_path_and_sample():
     sample = pd.read_csv(golden("sample4800.csv"))["sample"].values
     g, o = _pair(obs, z, grid, VGM_PC2D, 1, path, sample)
     e = _check(g, o, float(np.ptp(z)), 1)
+    cnt = g.gpu_counters()
+    assert cnt["sim_one_launch"] == 1 and cnt["sim_levels"] > 1  # every level in one launch
     sims, _ = g.get_results()
     assert sims.shape == (len(grid),)
     sims_m, _ = g.get_results(squeeze=False)
