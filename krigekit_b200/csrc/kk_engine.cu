@@ -684,8 +684,11 @@ void engine_solve(Engine& e) {
       // the systems of a sequential simulation: every target searches the
       // observations and the targets visited before it (exact kd-tree order)
       if (S.mode != 0 && !d.tree_ready) build_tree(e, v);
-      const int nthreads = std::max(1, std::min(nb, 32768));
+      // a thread per target up to the heap memory of 262 144 threads (one
+      // round: a second round on part of the threads doubles the launch)
       const int stride = (S.mode == 2 ? S.K : S.nmax) + 2;
+      const long long cap = std::max(32768LL, (long long)((size_t(1) << 30) / (kd_heap_entry_bytes() * stride)));
+      const int nthreads = (int)std::max(1LL, std::min<long long>({(long long)nb, 262144LL, cap}));
       DBuf heaps;
       heaps.reserve(kd_heap_entry_bytes() * (size_t)stride * nthreads);
       timer.start();
