@@ -127,9 +127,13 @@ int krige_get_estimate(int64_t handle, int nsim_c, int nblocks, double *out);
 /* kriging_capi.F90:410-443 krige_set_sim: SGSIM visiting order randpath(nblocks), 1-based,
  * and N(0, 1) draws sample(nsim_c, nvar_c, nblocks) of the p-th visited target; either
  * pointer may be NULL (a seeded random order / draws, not the reference's generator).
- * One variable, point targets, no sector search or external drift. */
+ * One variable and point targets; sector search and external drift as in kriging. */
 int krige_set_sim(int64_t handle, int nblocks, const int *randpath, int nsim_c, int nvar_c,
                   const double *sample);
+/* No counterpart in the reference.  How a simulation draws its values: 0 (default) every
+ * dependency level in one cooperative launch, 1 one launch per level.  Both give the same
+ * values bit for bit. */
+int krige_set_sim_draw(int64_t handle, int by_level);
 /* No counterpart in the reference.  Neighbour sets of the last sequential simulation:
  * nnear(2, nblocks) = observation and simulated members; inear(mmax, nblocks), 0-based, in
  * each target's system order: observations (< nobs), then nobs + visiting position. */

@@ -90,6 +90,7 @@ SIGNATURES = {
     "krige_set_autotune": ([_c_i64, _c_int], _c_int),
     "krige_set_sim": ([_c_i64, _c_int, ctypes.c_void_p, _c_int, _c_int, ctypes.c_void_p], _c_int),
     "krige_get_sim_neighbours": ([_c_i64, _c_int, _c_int, _p_int, _p_int], _c_int),
+    "krige_set_sim_draw": ([_c_i64, _c_int], _c_int),
     "krige_get_kernel_plan": ([_c_i64, _p_int, _p_dbl], _c_int),
     "krige_autotune_clear": ([], _c_int),
     "krige_gpu_phases": ([_c_i64, _p_dbl, _p_int], _c_int),

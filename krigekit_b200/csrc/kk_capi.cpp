@@ -722,6 +722,17 @@ int krige_get_sim_neighbours(int64_t h, int nblocks, int mmax, int* nnear, int* 
   KK_GUARD_END
 }
 
+// How a simulation draws its values (no reference counterpart): 0 one
+// cooperative launch for every level, 1 one launch per level.
+int krige_set_sim_draw(int64_t h, int by_level) {
+  KK_GUARD_BEGIN
+  Engine* e = get(h);
+  if (!e) return 1;
+  if (by_level != 0 && by_level != 1) throw std::string("by_level must be 0 or 1");
+  e->sim_by_level = by_level;
+  KK_GUARD_END
+}
+
 // krige_set_sim, kriging_capi.F90:410-443 -> set_sim_base (kriging_base.F90:1226-1320):
 // randpath (nblocks, 1-based) and sample (nsim, nvar, nblocks), either may be NULL
 int krige_set_sim(int64_t h, int nblocks, const int* randpath, int nsim_c, int nvar_c, const double* sample) {

@@ -1515,7 +1515,7 @@ static void engine_sgsim(Engine& e) {
   dflags.reserve(sizeof(int) * ((size_t)nb + 2));
   KK_CUDA(cudaMemsetAsync(dflags.p, 0, sizeof(int) * ((size_t)nb + 2), st));
   int* flags = dflags.as<int>();
-  bool flow = launch_sgsim_flow(SP, dorder.as<int>(), nb, flags, flags + nb, flags + nb + 1, nsm, st);
+  bool flow = !e.sim_by_level && launch_sgsim_flow(SP, dorder.as<int>(), nb, flags, flags + nb, flags + nb + 1, nsm, st);
   int nlaunch = 1;
   if (flow) {
     KK_CUDA(cudaGetLastError());

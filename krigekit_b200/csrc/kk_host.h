@@ -186,6 +186,7 @@ struct Engine {
   int sim_nobs = -1;
   int sim_levels = 0;  // dependency levels of the last simulation
   int sim_flow = 0;    // 1 when its draws ran as one launch (k_sgsim_flow)
+  int sim_by_level = 0;  // 1: draw level by level (k_sgsim_level) instead
   // neighbour sets of the last simulation by target: counts (observation,
   // simulated) and lists (sim_mmax per target; observations < nobs, then
   // nobs + visiting position), in the order of the target's system

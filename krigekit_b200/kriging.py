@@ -290,6 +290,12 @@ class Kriging:
                   float(dip), float(plunge), int(bool(sector_search)))
 
     # -------------------------------------------------------------------- solve
+    def set_sim_draw(self, by_level: bool = False):
+        """How the simulation draws its values (extension): every dependency
+        level in one launch (default) or one launch per level; the values are
+        the same bit for bit."""
+        _lib.call("krige_set_sim_draw", self._h(), int(bool(by_level)))
+
     def set_sim(self, randpath: Optional[np.ndarray] = None, sample: Optional[np.ndarray] = None):
         """Sequential Gaussian simulation: visiting order and N(0, 1) draws
         (kriging.py:1134-1203).  randpath is a 1-based permutation of the

@@ -272,3 +272,29 @@ def test_sgsim_3d_rangescale_and_local_nugget():
     g.solve()
     o.solve()
     _check(g, o, float(np.ptp(z)), 1)
+
+
+def test_sgsim_one_launch_equals_level_by_level():
+    """The one-launch draw (k_sgsim_flow) and the level-by-level launches
+    (k_sgsim_level) give the same realisations bit for bit."""
+    from krigekit_b200 import Kriging
+    obs, z, grid = _pc2d()
+    rng = np.random.default_rng(17)
+    path = rng.permutation(len(grid)) + 1
+    sample = rng.normal(0, 1, (len(grid), 3))
+    out = []
+    for by_level in (False, True):
+        k = Kriging(ndim=2, nvar=1, nsim=3)
+        k.set_obs(1, obs, z, nmax=16)
+        k.set_vgm(1, 1, **VGM_PC2D)
+        k.set_grid(grid)
+        k.set_search(1)
+        k.set_sim(path, sample)
+        k.set_sim_draw(by_level)
+        k.solve()
+        cnt = k.gpu_counters()
+        assert cnt["sim_one_launch"] == (0 if by_level else 1)
+        out.append(np.asarray(k.get_results(squeeze=False)[0]).copy())
+        k.close()
+    np.testing.assert_array_equal(out[0], out[1])
+    assert np.isfinite(out[0]).all()
