@@ -582,7 +582,17 @@ void engine_solve(Engine& e) {
     KkGrid keep_grid = d.search.grid;
     KkTree keep_tree = d.search.tree;
     d.search = S;
-    if (S.mode != 0) {
+    if (S.mode != 0 && e.sim_nobs >= 0) {
+      // the systems of a simulation search the kd-tree only: its search
+      // coordinates, without the grid
+      d.search.grid.D = D;  // k_search_coords writes D coordinates
+      d.tree_rdata.reserve(sizeof(double) * (size_t)D * S.nobs);
+      const double* xs[4] = {d.x[0].as<double>(), d.x[1].as<double>(), d.x[2].as<double>(), d.x[3].as<double>()};
+      launch_search_coords(d.search, xs, d.tree_rdata.as<double>(), S.nobs, st);
+      KK_CUDA(cudaGetLastError());
+      d.grid_ready = false;
+      d.tree_ready = false;
+    } else if (S.mode != 0) {
       if (rebuild) build_grid(e, v);
       else { d.search.grid = keep_grid; d.search.tree = keep_tree; }
     } else {
