@@ -275,41 +275,67 @@ void build_models(const Engine& e, std::vector<KkModel>& mdl, std::vector<KkSTMo
 // reference (kdtree2_maxidx.f90:629-916): mean split on the dimension of
 // largest spread, bucket size 12, boxes refined from the children.
 // ---------------------------------------------------------------------------
+#ifndef KK_KD_SPLIT_MIN
+#define KK_KD_SPLIT_MIN (1 << 14)  // points from which subtrees build in threads
+#endif
+
 namespace {
+constexpr int KD_EXT = -2;  // the parent is a node of another builder (a subtree's root)
+
 struct TreeBuild {
-  const double* data;  // (D, n) point-major
-  int D, n;
-  std::vector<int> ind;
+  int D = 0;
+  int* ind = nullptr;     // shared by every builder: disjoint ranges
+  // the points in the order of ind (row i = data row ind[i]): every pass over
+  // a node's range reads them in sequence instead of gathering
+  double* pts = nullptr;
   std::vector<int> ni;      // 5 per node
   std::vector<double> nd;   // 3 per node
   std::vector<double> box;  // 2*D per node
-  double v(int c, int i) const { return data[(size_t)i * D + c]; }
+  // the parent of a subtree's root, in the builder above it
+  int ext_cut = -1;
+  const double* ext_box = nullptr;
+  // the builder above the subtrees: ranges left for them, and the nodes whose
+  // boxes wait for their children
+  struct Job { int l, u, parent, side; };
+  int split_depth = -1;
+  std::vector<Job> jobs;
+  std::vector<int> pending;
+
+  double v(int c, int i) const { return pts[(size_t)i * D + c]; }  // coordinate c of range position i
 
   void spread(int c, int l, int u, double& smin, double& smax) const {
-    smin = v(c, ind[l]);
+    smin = v(c, l);
     smax = smin;
     int i;
     for (i = l + 2; i <= u; i += 2) {
-      double lmin = v(c, ind[i - 1]), lmax = v(c, ind[i]);
+      double lmin = v(c, i - 1), lmax = v(c, i);
       if (lmin > lmax) std::swap(lmin, lmax);
       if (smin > lmin) smin = lmin;
       if (smax < lmax) smax = lmax;
     }
     if (i == u + 1) {
-      double last = v(c, ind[u]);
+      double last = v(c, u);
       if (smin > last) smin = last;
       if (smax < last) smax = last;
     }
   }
+  void swap_pos(int a, int b) {
+    std::swap(ind[a], ind[b]);
+    for (int k = 0; k < D; ++k) std::swap(pts[(size_t)a * D + k], pts[(size_t)b * D + k]);
+  }
   int select_value(int c, double alpha, int lb, int rb) {
     while (lb < rb) {
-      if (v(c, ind[lb]) <= alpha) ++lb;
-      else { std::swap(ind[lb], ind[rb]); --rb; }
+      if (v(c, lb) <= alpha) ++lb;
+      else { swap_pos(lb, rb); --rb; }
     }
-    return v(c, ind[lb]) <= alpha ? lb : lb - 1;
+    return v(c, lb) <= alpha ? lb : lb - 1;
   }
-  int node(int l, int u, int parent) {
+  int node(int l, int u, int parent, int depth = 0, int side = 0) {
     if (u < l) return -1;
+    if (depth == split_depth) {  // left for a subtree builder
+      jobs.push_back({l, u, parent, side});
+      return -1;
+    }
     int me = (int)(ni.size() / 5);
     ni.resize(ni.size() + 5);
     nd.resize(nd.size() + 3);
@@ -325,10 +351,12 @@ struct TreeBuild {
       nd[me * 3 + 0] = 0.0;
       return me;
     }
+    const int pcut = parent >= 0 ? ni[parent * 5 + 0] : (parent == KD_EXT ? ext_cut : -1);
+    const double* pbox = parent >= 0 ? &box[(size_t)parent * 2 * D] : (parent == KD_EXT ? ext_box : nullptr);
     for (int i = 0; i < D; ++i) {
-      if (parent >= 0 && i != ni[parent * 5 + 0]) {
-        box[(size_t)me * 2 * D + 2 * i] = box[(size_t)parent * 2 * D + 2 * i];
-        box[(size_t)me * 2 * D + 2 * i + 1] = box[(size_t)parent * 2 * D + 2 * i + 1];
+      if (pbox && i != pcut) {
+        box[(size_t)me * 2 * D + 2 * i] = pbox[2 * i];
+        box[(size_t)me * 2 * D + 2 * i + 1] = pbox[2 * i + 1];
       } else {
         double lo, hi;
         spread(i, l, u, lo, hi);
@@ -343,15 +371,22 @@ struct TreeBuild {
       if (s > best) { best = s; c = i; }
     }
     double sum = 0.0;
-    for (int i = l; i <= u; ++i) sum = sum + v(c, ind[i]);
+    for (int i = l; i <= u; ++i) sum = sum + v(c, i);
     double average = sum / (double)(u - l + 1);
     nd[me * 3 + 0] = average;
     int m = select_value(c, average, l, u);
     ni[me * 5 + 0] = c;
-    int left = node(l, m, me);
-    int right = node(m + 1, u, me);
+    int left = node(l, m, me, depth + 1, 3);
+    int right = node(m + 1, u, me, depth + 1, 4);
     ni[me * 5 + 3] = left;
     ni[me * 5 + 4] = right;
+    if (split_depth >= 0) pending.push_back(me);  // children may still be subtrees
+    else refine(me);
+    return me;
+  }
+  // the box and split bounds of node me from its children
+  void refine(int me) {
+    const int c = ni[me * 5 + 0], left = ni[me * 5 + 3], right = ni[me * 5 + 4];
     double* b = &box[(size_t)me * 2 * D];
     if (right < 0) {
       for (int i = 0; i < 2 * D; ++i) b[i] = box[(size_t)left * 2 * D + i];
@@ -370,7 +405,6 @@ struct TreeBuild {
         b[2 * i] = std::fmin(box[(size_t)left * 2 * D + 2 * i], box[(size_t)right * 2 * D + 2 * i]);
       }
     }
-    return me;
   }
 };
 }  // namespace
@@ -378,20 +412,52 @@ struct TreeBuild {
 void build_kdtree(const double* data, int D, int n, std::vector<int>& node_i,
                   std::vector<double>& node_d, std::vector<double>& box, std::vector<int>& ind,
                   std::vector<double>& rdata, int& root) {
+  ind.resize(n);
+  for (int i = 0; i < n; ++i) ind[i] = i;
+  rdata.assign(data, data + (size_t)D * n);  // becomes the points in tree order
   TreeBuild t;
-  t.data = data;
   t.D = D;
-  t.n = n;
-  t.ind.resize(n);
-  for (int i = 0; i < n; ++i) t.ind[i] = i;
+  t.ind = ind.data();
+  t.pts = rdata.data();
+  // large sets: the nodes above depth 3 here, the (up to) eight subtrees below
+  // them in threads over their disjoint ranges, then merged and the upper
+  // boxes refined from their children (the same tree as a serial build)
+  t.split_depth = n >= KK_KD_SPLIT_MIN ? 3 : -1;
   root = t.node(0, n - 1, -1);
+  if (!t.jobs.empty()) {
+    std::vector<TreeBuild> sub(t.jobs.size());
+    std::vector<std::vector<double>> pbox(t.jobs.size());
+    for (size_t j = 0; j < t.jobs.size(); ++j) {
+      const TreeBuild::Job& jb = t.jobs[j];
+      TreeBuild& b = sub[j];
+      b.D = D;
+      b.ind = t.ind;
+      b.pts = t.pts;
+      b.ext_cut = t.ni[jb.parent * 5 + 0];
+      pbox[j].assign(&t.box[(size_t)jb.parent * 2 * D], &t.box[(size_t)jb.parent * 2 * D] + 2 * D);
+      b.ext_box = pbox[j].data();
+    }
+    std::vector<int> sroot(t.jobs.size(), -1);
+    par_for(t.jobs.size(), 1, [&](size_t j0, size_t j1) {
+      for (size_t j = j0; j < j1; ++j) sroot[j] = sub[j].node(t.jobs[j].l, t.jobs[j].u, KD_EXT);
+    });
+    for (size_t j = 0; j < t.jobs.size(); ++j) {
+      const int off = (int)(t.ni.size() / 5);
+      const TreeBuild& b = sub[j];
+      for (size_t k = 0; k < b.ni.size(); ++k) {
+        int x = b.ni[k];
+        if ((k % 5 == 3 || k % 5 == 4) && x >= 0) x += off;
+        t.ni.push_back(x);
+      }
+      t.nd.insert(t.nd.end(), b.nd.begin(), b.nd.end());
+      t.box.insert(t.box.end(), b.box.begin(), b.box.end());
+      t.ni[t.jobs[j].parent * 5 + t.jobs[j].side] = sroot[j] >= 0 ? sroot[j] + off : -1;
+    }
+  }
+  for (int me : t.pending) t.refine(me);  // listed after their children (post-order)
   node_i.swap(t.ni);
   node_d.swap(t.nd);
   box.swap(t.box);
-  rdata.resize((size_t)D * n);
-  for (int i = 0; i < n; ++i)
-    for (int d = 0; d < D; ++d) rdata[(size_t)i * D + d] = data[(size_t)t.ind[i] * D + d];
-  ind.swap(t.ind);
 }
 
 }  // namespace kk
